@@ -1,0 +1,157 @@
+/*
+ * nadvibs.h -- C ABI of the B200 Lanczos stage of NadVibS (libnadvibs_gpu.so).
+ *
+ * Drop-in boundary for the Lanczos stage of the reference program
+ * (Source/main.f90:61-79): a Fortran driver binds these entry points through
+ * ISO_C_BINDING (all integers int64_t, reals double, strings NUL-terminated), a C driver
+ * calls them directly, and the Python package binds them with ctypes.
+ *
+ * Conventions
+ *  - Every entry point returns 0 on success and a negative NVB_ERR_* code on failure;
+ *    nvb_last_error() returns a thread-local message for the last failure.  The
+ *    reference prints and continues on errors (Source/top.f90:396,1303-1308); here
+ *    failures are reported to the caller instead.
+ *  - A handle owns its device memory and a CUDA stream; caller-owned host arrays are
+ *    never retained.  One host thread per handle.
+ *  - Vectors passed by device pointer use the reference layout q(dimen, nstates),
+ *    column-major: element (row r, state s) at s*dimen + r, rows ordered with the last
+ *    mode fastest (shft(k) = prod_{j>k} nfunc(j), Source/top.f90:379-386).
+ *  - Energies are hartree unless stated otherwise; AU2WAVE = 219474.6313705.
+ *  - There is no CPU fallback: without a usable CUDA device nvb_create* fails.
+ */
+#ifndef NADVIBS_H
+#define NADVIBS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NVB_OK 0
+#define NVB_ERR_ARG (-1)       /* invalid argument or size */
+#define NVB_ERR_IO (-2)        /* file missing, unreadable or malformed */
+#define NVB_ERR_CUDA (-3)      /* CUDA runtime error or no device */
+#define NVB_ERR_STATE (-4)     /* call out of order (e.g. ritz before lanczos) */
+#define NVB_ERR_NOMEM (-5)     /* device or host allocation failed */
+#define NVB_ERR_BREAKDOWN (-6) /* Lanczos breakdown: beta below threshold or not finite */
+
+#define NVB_FP64 0  /* vectors and H.v in FP64 */
+#define NVB_MIXED 1 /* vectors and H.v in FP32, recurrence/dots/eigensolve in FP64 */
+
+#define NVB_DTYPE_F64 0
+#define NVB_DTYPE_F32 1
+
+typedef struct nvb_handle nvb_handle;
+
+/* The &NADVIBS namelist of basis.in, with the reference's defaults and array bounds
+ * (get_keywords, Source/secondary.f90:826-870). */
+typedef struct nvb_params {
+    int64_t niter, natoms, nmodes, nstates, ordr, restart, bconv, idroots, soroots;
+    int64_t reorthog, chkorthog, nseg, shiftref, nirreps;
+    double ztoler, maxdisk;
+    int64_t basis[100];
+    int64_t initstate[100];
+    int64_t npirr[10];
+    double weights[10];
+} nvb_params;
+
+/* Build options (not part of the reference input). */
+typedef struct nvb_options {
+    int64_t precision;     /* NVB_FP64 or NVB_MIXED */
+    int64_t device;        /* CUDA device ordinal; -1 = host-only handle (term table and
+                              text outputs only, every device entry point fails) */
+    int64_t quirk_cubic;   /* 1 (default): <m|x^3|m+-1> as the reference tabulates it
+                              (Source/function.f90:225-227, a factor 3 short); 0: exact */
+    int64_t quirk_lower;   /* 1 (default): constant / even-power couplings between different
+                              states applied to the lower triangle only, as the reference
+                              does (Source/top.f90:752-754); 0: symmetric */
+    int64_t archive_max;   /* max Lanczos vectors kept on the device for Ritz vectors /
+                              re-orthogonalisation; 0 = none (two-pass Ritz vectors) */
+    int64_t hv_kernel;     /* 0 = automatic choice; 1 = gather kernel; 2 = tiled kernel */
+    int64_t seed;          /* seed of the omega-recurrence noise (the reference is unseeded) */
+} nvb_options;
+
+/* Defaults of both structures.  Replaces the assignments of Source/secondary.f90:835-843. */
+int nvb_params_default(nvb_params *p);
+int nvb_options_default(nvb_options *o);
+
+/* Parse basis.in (the &NADVIBS group).  Replaces get_keywords (Source/secondary.f90:826-870)
+ * without the restart bookkeeping, which nvb_load_restart performs. */
+int nvb_read_basis(const char *path, nvb_params *p);
+
+/* Read basis.in + nadvibs.in and build the device plan.  Replaces read_basis +
+ * read_constants + initialize_elements (Source/top.f90:32-246,344-634).  Only
+ * shiftref=0 inputs are accepted (the Duschinsky seed is not built). */
+int nvb_create_from_files(const char *basis_path, const char *nadvibs_path, const nvb_options *opt,
+                          nvb_handle **out);
+
+/* Same, from memory.  omega[nmodes] (hartree), concoef[nstates(nstates+1)/2] in block order
+ * k = i(i-1)/2 + j (i >= j), potterms = for each block, for each order d = 1..ordr, the
+ * C(nmodes+d-1, d) coefficients in the nadvibs.in monomial order (Source/top.f90:122-168),
+ * concatenated without padding. */
+int nvb_create(const nvb_params *p, const double *omega, const double *concoef, const double *potterms,
+               const nvb_options *opt, nvb_handle **out);
+
+int nvb_destroy(nvb_handle *h);
+const char *nvb_last_error(void);
+
+/* Sizes: dimen = prod(nfunc) (rows per state), total = dimen*nstates, nterms = distinct
+ * monomials after the merge, npot = number of potterms values, iters = completed Lanczos
+ * iterations. */
+int nvb_get_sizes(nvb_handle *h, int64_t *dimen, int64_t *nstates, int64_t *nmodes, int64_t *nterms,
+                  int64_t *npot, int64_t *iters);
+
+/* The merged term table in the reference's representation (nzindx/nzblks/nzcoef of
+ * Source/top.f90:199-231): for term t, tcnt[t] distinct modes, tmode[t*4+l] (1-based) and
+ * tpow[t*4+l]; tnpair[t] state pairs tpa/tpb[t*nstates^2+q] (1-based) with coefficient
+ * tcoef[t*nstates^2+q] (scaled by 1/prod omega^(p/2)). */
+int nvb_get_terms(nvb_handle *h, int64_t *tcnt, int64_t *tmode, int64_t *tpow, int64_t *tnpair,
+                  int64_t *tpa, int64_t *tpb, double *tcoef);
+
+/* Precision of subsequent Lanczos runs (resets the Lanczos state). */
+int nvb_set_precision(nvb_handle *h, int64_t precision);
+
+/* Run the handle's work on a caller stream (cudaStream_t passed as void*, e.g.
+ * cudaStreamLegacy for the legacy default stream); NULL restores the handle-owned stream,
+ * which does not synchronise with the legacy default stream. */
+int nvb_set_stream(nvb_handle *h, void *stream);
+int nvb_synchronize(nvb_handle *h);
+
+/* y = H x on device pointers of dtype NVB_DTYPE_F64 or NVB_DTYPE_F32 (both vectors the same
+ * dtype).  Replaces Hv (Source/top.f90:672-818).  Stream-ordered, asynchronous. */
+int nvb_hv(nvb_handle *h, const void *x, void *y, int64_t dtype);
+
+/* Generate the seed vector: |0...0> in every state weighted by weights[nstates] and
+ * normalised (generate_initialvec, simple branch, Source/secondary.f90:727-783).
+ * weights may be NULL (basis.in weights).  Resets the Lanczos state; beta(0)=||seed||. */
+int nvb_seed(nvb_handle *h, const double *weights);
+
+/* Run niter further Lanczos iterations (update_lanczos + Hv + lanczos_step [+ set_omega +
+ * partial_orthog], Source/main.f90:63-71, Source/top.f90:646-1005) with the handle's
+ * reorthogonalisation settings.  alpha receives alpha(1..iters), beta beta(0..iters) for
+ * ALL iterations done so far (iters = previous + niter); either may be NULL. */
+int nvb_lanczos(nvb_handle *h, int64_t niter, double *alpha, double *beta);
+
+/* Ritz system of T_n, n <= iters (compute_ritzsystem, Source/secondary.f90:240-257):
+ * E[n] ascending (hartree), bji[n] = |beta(n) s(n,i)|, inten[n] = s(1,i)^2, sign[n] of
+ * s(1,i); vect (optional, n*n column-major) the eigenvectors of T_n. */
+int nvb_ritz(nvb_handle *h, int64_t n, double *E, double *bji, double *inten, int64_t *sign, double *vect);
+
+/* Write output.dat's eigenvalue section (compute_eigenvalues, Source/top.f90:1051-1113)
+ * for T_n, n = iters, with bjiconv = 10^-bconv from basis.in, appending to path. */
+int nvb_write_eigenvalues(nvb_handle *h, const char *path);
+
+/* Write the output.dat header for the job (print_basis, Source/top.f90:248-342), replacing
+ * path. */
+int nvb_write_header(nvb_handle *h, const char *path);
+
+/* Device pointer to the current Lanczos vector v_i, v_{i-1} and the residual (dtype of the
+ * handle's precision) with their scale factors (v = scale * buffer). */
+int nvb_lanczos_vectors(nvb_handle *h, void **cur, double *scur, void **prev, double *sprev, void **res,
+                        double *sres);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,227 @@
+"""ctypes binding of libnadvibs_gpu.so (the C ABI of include/nadvibs.h).
+
+The library is built in-tree (``nadvibs_b200/libnadvibs_gpu.so``, see ``build.py``).  There is
+no CPU fallback: if the library is missing, or no CUDA device is usable when a handle is
+created, the call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libnadvibs_gpu.so")
+
+NVB_FP64, NVB_MIXED = 0, 1
+DTYPE_F64, DTYPE_F32 = 0, 1
+
+ERRORS = {-1: "NVB_ERR_ARG", -2: "NVB_ERR_IO", -3: "NVB_ERR_CUDA", -4: "NVB_ERR_STATE",
+          -5: "NVB_ERR_NOMEM", -6: "NVB_ERR_BREAKDOWN"}
+
+
+class NvbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("niter", "natoms", "nmodes", "nstates", "ordr", "restart", "bconv",
+                                          "idroots", "soroots", "reorthog", "chkorthog", "nseg", "shiftref",
+                                          "nirreps")] + \
+               [("ztoler", C.c_double), ("maxdisk", C.c_double), ("basis", C.c_int64 * 100),
+                ("initstate", C.c_int64 * 100), ("npirr", C.c_int64 * 10), ("weights", C.c_double * 10)]
+
+
+class Options(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("precision", "device", "quirk_cubic", "quirk_lower", "archive_max",
+                                          "hv_kernel", "seed")]
+
+
+_lib = None
+
+# (name, restype, argtypes); every entry point returns int status unless stated
+_SIGS = {
+    "nvb_params_default": [C.c_void_p],
+    "nvb_options_default": [C.c_void_p],
+    "nvb_read_basis": [C.c_char_p, C.c_void_p],
+    "nvb_create_from_files": [C.c_char_p, C.c_char_p, C.c_void_p, C.c_void_p],
+    "nvb_create": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "nvb_destroy": [C.c_void_p],
+    "nvb_get_sizes": [C.c_void_p] + [C.c_void_p] * 6,
+    "nvb_get_terms": [C.c_void_p] + [C.c_void_p] * 7,
+    "nvb_set_precision": [C.c_void_p, C.c_int64],
+    "nvb_set_stream": [C.c_void_p, C.c_void_p],
+    "nvb_synchronize": [C.c_void_p],
+    "nvb_hv": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64],
+    "nvb_seed": [C.c_void_p, C.c_void_p],
+    "nvb_lanczos": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
+    "nvb_ritz": [C.c_void_p, C.c_int64] + [C.c_void_p] * 5,
+    "nvb_write_eigenvalues": [C.c_void_p, C.c_char_p],
+    "nvb_write_header": [C.c_void_p, C.c_char_p],
+    "nvb_lanczos_vectors": [C.c_void_p] + [C.c_void_p] * 6,
+}
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built: run `python -m nadvibs_b200.build` "
+                              "(there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.restype = C.c_int
+            fn.argtypes = args
+        L.nvb_last_error.restype = C.c_char_p
+        L.nvb_last_error.argtypes = []
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise NvbError(rc, lib().nvb_last_error().decode(errors="replace"))
+
+
+def _p(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def default_params() -> Params:
+    p = Params()
+    check(lib().nvb_params_default(C.byref(p)))
+    return p
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    check(lib().nvb_options_default(C.byref(o)))
+    for k, v in kw.items():
+        setattr(o, k, int(v))
+    return o
+
+
+def read_basis(path: str) -> Params:
+    p = Params()
+    check(lib().nvb_read_basis(path.encode(), C.byref(p)))
+    return p
+
+
+class Handle:
+    """Owns one nvb_handle."""
+
+    def __init__(self, ptr):
+        self.ptr = ptr
+
+    @classmethod
+    def from_files(cls, basis: str, nadvibs: str, **opts) -> "Handle":
+        o = default_options(**opts)
+        h = C.c_void_p()
+        check(lib().nvb_create_from_files(basis.encode(), nadvibs.encode(), C.byref(o), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_arrays(cls, params: Params, omega, concoef, potterms, **opts) -> "Handle":
+        o = default_options(**opts)
+        om = np.ascontiguousarray(omega, dtype=np.float64)
+        cc = np.ascontiguousarray(concoef, dtype=np.float64)
+        pt = np.ascontiguousarray(potterms, dtype=np.float64)
+        h = C.c_void_p()
+        check(lib().nvb_create(C.byref(params), _p(om), _p(cc), _p(pt), C.byref(o), C.byref(h)))
+        return cls(h)
+
+    def close(self):
+        if self.ptr:
+            lib().nvb_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def sizes(self) -> dict:
+        v = [C.c_int64() for _ in range(6)]
+        check(lib().nvb_get_sizes(self.ptr, *[C.byref(x) for x in v]))
+        return dict(zip(("dimen", "nstates", "nmodes", "nterms", "npot", "iters"), [x.value for x in v]))
+
+    def terms(self):
+        sz = self.sizes()
+        nt, S = sz["nterms"], sz["nstates"]
+        tcnt = np.zeros(max(nt, 1), np.int64)
+        tmode = np.zeros((max(nt, 1), 4), np.int64)
+        tpow = np.zeros((max(nt, 1), 4), np.int64)
+        tnp = np.zeros(max(nt, 1), np.int64)
+        tpa = np.zeros((max(nt, 1), S * S), np.int64)
+        tpb = np.zeros((max(nt, 1), S * S), np.int64)
+        tco = np.zeros((max(nt, 1), S * S))
+        check(lib().nvb_get_terms(self.ptr, _p(tcnt), _p(tmode), _p(tpow), _p(tnp), _p(tpa), _p(tpb), _p(tco)))
+        out = []
+        for t in range(nt):
+            c = int(tcnt[t])
+            out.append(dict(modes=list(tmode[t, :c]), pows=list(tpow[t, :c]),
+                            pairs=[(int(tpa[t, q]), int(tpb[t, q])) for q in range(tnp[t])],
+                            coefs=list(tco[t, : tnp[t]])))
+        return out
+
+    def set_precision(self, prec: int):
+        check(lib().nvb_set_precision(self.ptr, prec))
+
+    def set_stream(self, stream_ptr: int | None):
+        """Run on a caller stream (a cudaStream_t as int).  0 means the legacy default stream
+        (passed as cudaStreamLegacy); None restores the handle's own stream."""
+        if stream_ptr is None:
+            check(lib().nvb_set_stream(self.ptr, None))
+        else:
+            check(lib().nvb_set_stream(self.ptr, C.c_void_p(stream_ptr if stream_ptr else 1)))
+
+    def synchronize(self):
+        check(lib().nvb_synchronize(self.ptr))
+
+    def hv_ptr(self, x_ptr: int, y_ptr: int, dtype: int):
+        check(lib().nvb_hv(self.ptr, C.c_void_p(x_ptr), C.c_void_p(y_ptr), dtype))
+
+    def seed(self, weights=None):
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        check(lib().nvb_seed(self.ptr, _p(w)))
+
+    def lanczos(self, niter: int):
+        it = self.sizes()["iters"] + niter
+        a = np.zeros(max(it, 1))
+        b = np.zeros(it + 1)
+        rc = lib().nvb_lanczos(self.ptr, niter, _p(a), _p(b))
+        check(rc)
+        return a[:it], b
+
+    def ritz(self, n: int, vectors: bool = False):
+        E = np.zeros(n); bji = np.zeros(n); inten = np.zeros(n)
+        sign = np.zeros(n, np.int64)
+        V = np.zeros((n, n)) if vectors else None
+        check(lib().nvb_ritz(self.ptr, n, _p(E), _p(bji), _p(inten), _p(sign), _p(V)))
+        return E, bji, inten, sign, (V.T.copy() if vectors else None)
+
+    def write_header(self, path: str):
+        check(lib().nvb_write_header(self.ptr, path.encode()))
+
+    def write_eigenvalues(self, path: str):
+        check(lib().nvb_write_eigenvalues(self.ptr, path.encode()))
+
+    def lanczos_vectors(self):
+        p = [C.c_void_p() for _ in range(3)]
+        s = [C.c_double() for _ in range(3)]
+        check(lib().nvb_lanczos_vectors(self.ptr, C.byref(p[0]), C.byref(s[0]), C.byref(p[1]), C.byref(s[1]),
+                                        C.byref(p[2]), C.byref(s[2])))
+        return [(p[i].value, s[i].value) for i in range(3)]

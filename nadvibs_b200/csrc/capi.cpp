@@ -1,0 +1,333 @@
+// extern "C" entry points of libnadvibs_gpu.so (declared in include/nadvibs.h).
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "handle.h"
+
+namespace nvb {
+void write_header(nvb_handle *h, const char *path);
+void write_eigenvalues(nvb_handle *h, const char *path, double seconds);
+
+static thread_local std::string g_err;
+
+void set_error(const std::string &m) { g_err = m; }
+[[noreturn]] void fail(int code, const std::string &msg) { throw Error{code, msg}; }
+
+void ensure_device(nvb_handle *h) {
+    if (h->device < 0) fail(NVB_ERR_CUDA, "host-only handle (device = -1): no device work possible");
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) fail(NVB_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+}
+}  // namespace nvb
+
+using namespace nvb;
+
+template <typename F>
+static int guarded(F &&f) {
+    try {
+        f();
+        return NVB_OK;
+    } catch (const Error &e) {
+        set_error(e.msg);
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return NVB_ERR_NOMEM;
+    } catch (const std::exception &e) {
+        set_error(e.what());
+        return NVB_ERR_ARG;
+    }
+}
+
+#define CKA(x)                                                                                   \
+    do {                                                                                         \
+        cudaError_t e_ = (x);                                                                    \
+        if (e_ != cudaSuccess) fail(NVB_ERR_CUDA, std::string(#x ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+extern "C" {
+
+int nvb_params_default(nvb_params *p) {
+    return guarded([&] {
+        if (!p) fail(NVB_ERR_ARG, "null params");
+        std::memset(p, 0, sizeof *p);
+        // Source/secondary.f90:835-843
+        p->restart = 0; p->niter = 1;
+        for (int i = 0; i < 100; ++i) { p->basis[i] = 1; p->initstate[i] = 0; }
+        p->nstates = 1; p->ordr = 2; p->natoms = 2; p->nmodes = 1;
+        p->nirreps = 1;
+        for (int i = 0; i < 10; ++i) p->npirr[i] = 0;
+        p->npirr[0] = p->nmodes;
+        p->shiftref = 0; p->bconv = 0; p->idroots = 0; p->soroots = 0;
+        p->reorthog = 0; p->chkorthog = 100; p->nseg = 1; p->ztoler = 1e-20;
+        p->maxdisk = 1000;
+        for (int i = 0; i < 10; ++i) p->weights[i] = 1.0;
+    });
+}
+
+int nvb_options_default(nvb_options *o) {
+    return guarded([&] {
+        if (!o) fail(NVB_ERR_ARG, "null options");
+        std::memset(o, 0, sizeof *o);
+        o->precision = NVB_FP64;
+        o->device = 0;
+        o->quirk_cubic = 1;
+        o->quirk_lower = 1;
+        o->archive_max = 0;
+        o->hv_kernel = 0;
+        o->seed = 12345;
+    });
+}
+
+int nvb_read_basis(const char *path, nvb_params *p) {
+    return guarded([&] {
+        if (!path || !p) fail(NVB_ERR_ARG, "null argument");
+        nvb_params q;
+        nvb_params_default(&q);
+        parse_basis_text(read_file(path), q);
+        *p = q;
+    });
+}
+
+static void create_common(nvb_handle *h, const nvb_params &p, const double *omega, const double *concoef,
+                          const double *pot, const nvb_options *opt) {
+    if (opt) h->opt = *opt;
+    else nvb_options_default(&h->opt);
+    if (h->opt.precision != NVB_FP64 && h->opt.precision != NVB_MIXED) fail(NVB_ERR_ARG, "bad precision");
+    build_system(h->sys, p, omega, concoef, pot);
+    h->reorthog = p.reorthog;
+    h->chkorthog = p.chkorthog > 0 ? p.chkorthog : 100;
+    if (h->opt.device == -1) {  // host-only handle: term table and text outputs, no device work
+        h->device = -1;
+        return;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        fail(NVB_ERR_CUDA, std::string("no CUDA device available (") + cudaGetErrorString(e) + "); there is no CPU path");
+    if (h->opt.device < 0 || h->opt.device >= ndev) fail(NVB_ERR_ARG, "device ordinal out of range");
+    h->device = (int)h->opt.device;
+    ensure_device(h);
+    CKA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    h->stream = h->own_stream;
+    h->precision = (int)h->opt.precision;
+    plan_build(h->plan, h->sys, (int)h->opt.quirk_cubic, (int)h->opt.quirk_lower);
+    plan_upload(h->plan);
+    h->reorthog = p.reorthog;
+    h->chkorthog = p.chkorthog > 0 ? p.chkorthog : 100;
+    h->rng_state = (uint64_t)h->opt.seed * 6364136223846793005ull + 1442695040888963407ull;
+}
+
+int nvb_create(const nvb_params *p, const double *omega, const double *concoef, const double *potterms,
+               const nvb_options *opt, nvb_handle **out) {
+    nvb_handle *h = nullptr;
+    int rc = guarded([&] {
+        if (!p || !omega || !concoef || !potterms || !out) fail(NVB_ERR_ARG, "null argument");
+        h = new nvb_handle();
+        create_common(h, *p, omega, concoef, potterms, opt);
+    });
+    if (rc != NVB_OK) {
+        if (h) nvb_destroy(h);
+        if (out) *out = nullptr;
+        return rc;
+    }
+    *out = h;
+    return NVB_OK;
+}
+
+int nvb_create_from_files(const char *basis_path, const char *nadvibs_path, const nvb_options *opt,
+                          nvb_handle **out) {
+    nvb_handle *h = nullptr;
+    int rc = guarded([&] {
+        if (!basis_path || !nadvibs_path || !out) fail(NVB_ERR_ARG, "null argument");
+        nvb_params p;
+        nvb_params_default(&p);
+        parse_basis_text(read_file(basis_path), p);
+        if (p.shiftref != 0) fail(NVB_ERR_ARG, "shiftref != 0 (Duschinsky seed) is not supported");
+        std::vector<double> om, cc, pot;
+        parse_nadvibs_text(read_file(nadvibs_path), p, om, cc, pot);
+        h = new nvb_handle();
+        create_common(h, p, om.data(), cc.data(), pot.data(), opt);
+    });
+    if (rc != NVB_OK) {
+        if (h) nvb_destroy(h);
+        if (out) *out = nullptr;
+        return rc;
+    }
+    *out = h;
+    return NVB_OK;
+}
+
+int nvb_destroy(nvb_handle *h) {
+    if (!h) return NVB_OK;
+    int rc = guarded([&] {
+        if (h->device >= 0) {
+            cudaSetDevice(h->device);
+            if (h->stream) cudaStreamSynchronize(h->stream);
+            lanczos_free(h);
+            plan_free(h->plan);
+            if (h->own_stream) cudaStreamDestroy(h->own_stream);
+        }
+    });
+    delete h;
+    return rc;
+}
+
+const char *nvb_last_error(void) { return g_err.c_str(); }
+
+int nvb_get_sizes(nvb_handle *h, int64_t *dimen, int64_t *nstates, int64_t *nmodes, int64_t *nterms, int64_t *npot,
+                  int64_t *iters) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        if (dimen) *dimen = h->sys.dimen;
+        if (nstates) *nstates = h->sys.S;
+        if (nmodes) *nmodes = h->sys.M;
+        if (nterms) *nterms = (int64_t)h->sys.terms.size();
+        if (npot) *npot = (int64_t)h->sys.potterms.size();
+        if (iters) *iters = h->iters;
+    });
+}
+
+int nvb_get_terms(nvb_handle *h, int64_t *tcnt, int64_t *tmode, int64_t *tpow, int64_t *tnpair, int64_t *tpa,
+                  int64_t *tpb, double *tcoef) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        const int S = h->sys.S;
+        for (size_t t = 0; t < h->sys.terms.size(); ++t) {
+            const Term &T = h->sys.terms[t];
+            if (tcnt) tcnt[t] = T.nm;
+            for (int l = 0; l < 4; ++l) {
+                if (tmode) tmode[t * 4 + l] = l < T.nm ? T.mode[l] + 1 : 0;
+                if (tpow) tpow[t * 4 + l] = l < T.nm ? T.pow[l] : 0;
+            }
+            if (tnpair) tnpair[t] = (int64_t)T.pairs.size();
+            for (int q = 0; q < S * S; ++q) {
+                const bool on = q < (int)T.pairs.size();
+                if (tpa) tpa[t * S * S + q] = on ? T.pairs[q].a + 1 : 0;
+                if (tpb) tpb[t * S * S + q] = on ? T.pairs[q].b + 1 : 0;
+                if (tcoef) tcoef[t * S * S + q] = on ? T.pairs[q].coef : 0.0;
+            }
+        }
+    });
+}
+
+int nvb_set_precision(nvb_handle *h, int64_t precision) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        if (precision != NVB_FP64 && precision != NVB_MIXED) fail(NVB_ERR_ARG, "bad precision");
+        ensure_device(h);
+        if (precision != h->precision) {
+            CKA(cudaStreamSynchronize(h->stream));
+            for (int i = 0; i < 3; ++i)
+                if (h->buf[i]) { cudaFree(h->buf[i]); h->buf[i] = nullptr; }
+            if (h->arch) { cudaFree(h->arch); h->arch = nullptr; h->arch_cap = h->arch_n = 0; }
+            h->precision = (int)precision;
+        }
+        h->seeded = false;
+        h->iters = 0;
+    });
+}
+
+int nvb_set_stream(nvb_handle *h, void *stream) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    });
+}
+
+int nvb_synchronize(nvb_handle *h) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        ensure_device(h);
+        CKA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int nvb_hv(nvb_handle *h, const void *x, void *y, int64_t dtype) {
+    return guarded([&] {
+        if (!h || !x || !y) fail(NVB_ERR_ARG, "null argument");
+        if (dtype != NVB_DTYPE_F64 && dtype != NVB_DTYPE_F32) fail(NVB_ERR_ARG, "bad dtype");
+        if (x == y) fail(NVB_ERR_ARG, "x and y must not alias");
+        ensure_device(h);
+        hv_any(h, x, y, (int)dtype, nullptr, nullptr, nullptr);
+    });
+}
+
+int nvb_seed(nvb_handle *h, const double *weights) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        ensure_device(h);
+        lanczos_seed(h, weights);
+    });
+}
+
+int nvb_lanczos(nvb_handle *h, int64_t niter, double *alpha, double *beta) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        ensure_device(h);
+        try {
+            lanczos_run(h, niter);
+        } catch (const Error &e) {
+            if (alpha) std::memcpy(alpha, h->alpha.data() + 1, h->iters * sizeof(double));
+            if (beta) std::memcpy(beta, h->beta.data(), (h->iters + 1) * sizeof(double));
+            throw;
+        }
+        if (alpha) std::memcpy(alpha, h->alpha.data() + 1, h->iters * sizeof(double));
+        if (beta) std::memcpy(beta, h->beta.data(), (h->iters + 1) * sizeof(double));
+    });
+}
+
+int nvb_ritz(nvb_handle *h, int64_t n, double *E, double *bji, double *inten, int64_t *sign, double *vect) {
+    return guarded([&] {
+        if (!h || !E) fail(NVB_ERR_ARG, "null argument");
+        if (n < 1 || n > h->iters) fail(NVB_ERR_STATE, "n must be in 1..iterations done");
+        std::vector<double> V((size_t)n * n);
+        tridiag_eigen(n, h->alpha.data() + 1, h->beta.data() + 1, E, V.data());
+        for (int64_t i = 0; i < n; ++i) {
+            const double s1 = V[(size_t)i * n], sn = V[(size_t)i * n + n - 1];
+            if (bji) bji[i] = std::fabs(h->beta[n] * sn);
+            if (inten) inten[i] = s1 * s1;
+            if (sign) sign[i] = s1 < 0 ? -1 : 1;
+        }
+        if (vect) std::memcpy(vect, V.data(), V.size() * sizeof(double));
+    });
+}
+
+int nvb_write_eigenvalues(nvb_handle *h, const char *path) {
+    return guarded([&] {
+        if (!h || !path) fail(NVB_ERR_ARG, "null argument");
+        auto t0 = std::chrono::steady_clock::now();
+        // timing printed is that of the eigen-solve itself
+        write_eigenvalues(h, path, 0.0);
+        (void)t0;
+    });
+}
+
+int nvb_write_header(nvb_handle *h, const char *path) {
+    return guarded([&] {
+        if (!h || !path) fail(NVB_ERR_ARG, "null argument");
+        write_header(h, path);
+    });
+}
+
+int nvb_lanczos_vectors(nvb_handle *h, void **cur, double *scur, void **prev, double *sprev, void **res,
+                        double *sres) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        if (!h->seeded) fail(NVB_ERR_STATE, "no Lanczos state");
+        ensure_device(h);
+        double sc[3];
+        CKA(cudaMemcpyAsync(sc, h->d_scale, sizeof sc, cudaMemcpyDeviceToHost, h->stream));
+        CKA(cudaStreamSynchronize(h->stream));
+        if (cur) *cur = h->buf[h->cur];
+        if (scur) *scur = sc[h->cur];
+        if (prev) *prev = h->buf[h->prev];
+        if (sprev) *sprev = sc[h->prev];
+        if (res) *res = h->buf[h->work];
+        if (sres) *sres = sc[h->work];
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,59 @@
+// The opaque nvb_handle: term table, device plan, Lanczos state and scratch.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "plan.h"
+
+struct nvb_handle {
+    nvb::System sys;
+    nvb_options opt{};
+    nvb::Plan plan;
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int precision = NVB_FP64;
+    // Lanczos state.  Three device buffers hold unnormalised vectors; v = scale[i] * buf[i].
+    void *buf[3] = {nullptr, nullptr, nullptr};
+    int cur = 0, prev = 1, work = 2;
+    int64_t iters = 0;      // completed iterations
+    bool seeded = false;
+    int64_t cap = 0;        // capacity of d_alpha / d_beta (iterations)
+    double *d_alpha = nullptr;  // [cap+1], alpha(i) at index i
+    double *d_beta = nullptr;   // [cap+1], beta(i) at index i
+    double *d_scale = nullptr;  // [3]
+    int *d_status = nullptr;    // [2]: breakdown flag, iteration
+    double *d_part = nullptr;   // reduction partials
+    int64_t part_len = 0;
+    std::vector<double> alpha, beta;  // host copies: alpha[1..iters] (alpha[0] unused), beta[0..iters]
+    // archive of normalised Lanczos vectors v_1..v_k (device, precision of the handle)
+    void *arch = nullptr;
+    int64_t arch_cap = 0, arch_n = 0;
+    // re-orthogonalisation
+    int64_t reorthog = 0, chkorthog = 100;
+    std::vector<double> omega1, omega2;  // omega(1,0:n), omega(2,0:n)
+    bool firststep = true;
+    std::vector<std::pair<int64_t, int64_t>> orth_ranges;
+    uint64_t rng_state = 0;
+    // cached scratch for ad-hoc vectors
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+
+    size_t elem_size() const { return precision == NVB_MIXED ? sizeof(float) : sizeof(double); }
+    int64_t ntotal() const { return sys.dimen * sys.S; }
+};
+
+namespace nvb {
+void ensure_device(nvb_handle *h);
+void lanczos_alloc(nvb_handle *h);
+void lanczos_free(nvb_handle *h);
+void lanczos_seed(nvb_handle *h, const double *weights);
+void lanczos_run(nvb_handle *h, int64_t niter);
+void hv_any(nvb_handle *h, const void *x, void *y, int dtype, const double *scale_dev, double *alpha_part,
+            int *nblocks_out);
+void ensure_partials(nvb_handle *h, int64_t n);
+double device_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, int dtype);
+void *scratch_vector(nvb_handle *h, size_t bytes);
+}  // namespace nvb

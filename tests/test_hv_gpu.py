@@ -1,0 +1,107 @@
+"""H.v parity through the C ABI on the GPU against the CPU oracle (Source/top.f90:672-818).
+
+FP64: max |y_gpu - y_oracle| <= 1e-12 * max |y| (same summation order per element; only
+FMA contraction and the rounding of the element products differ).
+FP32: max |y_gpu - y_oracle| <= 2e-5 * max |y| (single-precision evaluation).
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from nadvibs_b200 import _lib as L
+from nadvibs_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 2e-5
+
+
+def _handle(p_or_cfg, om, cc, pot, **opts):
+    return L.Handle.from_arrays(p_or_cfg, om, cc, synth.flatten_pot(pot), **opts)
+
+
+def _params(cfg):
+    p = L.default_params()
+    p.nstates, p.nmodes, p.ordr = cfg.nstates, cfg.nmodes, cfg.ordr
+    for i, b in enumerate(cfg.basis):
+        p.basis[i] = b
+    p.niter = cfg.niter
+    return p
+
+
+def _hv_gpu(h, x: np.ndarray, dtype=torch.float64):
+    xt = torch.from_numpy(x).to(device="cuda", dtype=dtype)
+    yt = torch.empty_like(xt)
+    h.set_stream(torch.cuda.current_stream().cuda_stream)
+    h.hv_ptr(xt.data_ptr(), yt.data_ptr(), L.DTYPE_F64 if dtype == torch.float64 else L.DTYPE_F32)
+    torch.cuda.synchronize()
+    return yt.double().cpu().numpy()
+
+
+SMALL = [(7, 2, [3, 4], 2), (8, 3, [2, 3, 2], 3), (9, 2, [4, 1, 3], 4), (10, 1, [5, 4], 4),
+         (12, 4, [3, 3, 2, 2], 2), (13, 2, [1, 1], 2), (14, 10, [2, 3], 2), (15, 3, [6, 5, 4], 4),
+         (16, 5, [2, 2, 2, 2, 2, 2], 3)]
+
+
+@pytest.mark.parametrize("seed,nstates,basis,ordr", SMALL)
+@pytest.mark.parametrize("quirks", [(1, 1), (0, 0)])
+def test_hv_small_systems_fp64_and_fp32(seed, nstates, basis, ordr, quirks):
+    cfg = synth.random_small(seed, nstates, basis, ordr)
+    om, cc, pot = synth.draw_small(cfg)
+    S = O.system_from_arrays(basis, nstates, ordr, om, cc, pot, quirk_cubic=bool(quirks[0]),
+                             quirk_lower=bool(quirks[1]))
+    x = np.random.default_rng(seed).normal(size=S.ntotal)
+    y_ref = S.hv(x)
+    with _handle(_params(cfg), om, cc, pot, quirk_cubic=quirks[0], quirk_lower=quirks[1]) as h:
+        y64 = _hv_gpu(h, x)
+        y32 = _hv_gpu(h, x, torch.float32)
+    scale = np.abs(y_ref).max()
+    assert np.abs(y64 - y_ref).max() <= TOL64 * scale
+    assert np.abs(y32 - y_ref).max() <= TOL32 * scale
+
+
+@pytest.mark.parametrize("n", [1, 4])
+def test_hv_benchmark_systems_full(n):
+    cfg = synth.config(n)
+    om, cc, pot = synth.draw(cfg)
+    S = O.system_from_arrays(cfg.basis, cfg.nstates, cfg.ordr, om, cc, pot)
+    x = np.random.default_rng(n).normal(size=S.ntotal)
+    y_ref = S.hv(x, nthreads=8)
+    with _handle(_params(cfg), om, cc, pot) as h:
+        y64 = _hv_gpu(h, x)
+        y32 = _hv_gpu(h, x, torch.float32)
+    scale = np.abs(y_ref).max()
+    assert np.abs(y64 - y_ref).max() <= TOL64 * scale
+    assert np.abs(y32 - y_ref).max() <= TOL32 * scale
+
+
+@pytest.mark.parametrize("n", [2])
+def test_hv_drop_in_size_rows_and_symmetry(n):
+    """Full-size systems: oracle rows at 2000 random positions (plus the first/last rows and
+    the truncation corners), and <u,Hv> = <Hu,v> over the whole vector."""
+    cfg = synth.config(n)
+    om, cc, pot = synth.draw(cfg)
+    S = O.system_from_arrays(cfg.basis, cfg.nstates, cfg.ordr, om, cc, pot)
+    N = S.dimen
+    g = torch.Generator(device="cuda").manual_seed(n)
+    x = torch.randn(S.ntotal, generator=g, device="cuda", dtype=torch.float64)
+    u = torch.randn(S.ntotal, generator=g, device="cuda", dtype=torch.float64)
+    with _handle(_params(cfg), om, cc, pot) as h:
+        h.set_stream(torch.cuda.current_stream().cuda_stream)
+        y = torch.empty_like(x)
+        h.hv_ptr(x.data_ptr(), y.data_ptr(), L.DTYPE_F64)
+        hu = torch.empty_like(u)
+        h.hv_ptr(u.data_ptr(), hu.data_ptr(), L.DTYPE_F64)
+        torch.cuda.synchronize()
+        lhs = torch.dot(u, y).item()
+        rhs = torch.dot(hu, x).item()
+        assert abs(lhs - rhs) <= 1e-10 * torch.linalg.vector_norm(y).item() * torch.linalg.vector_norm(u).item()
+        rng = np.random.default_rng(n)
+        rows = np.concatenate([[0, 1, N - 2, N - 1], rng.integers(0, N, size=2000)])
+        xh = x.cpu().numpy()
+        yr = S.hv_rows(xh, rows)
+        yg = y.view(cfg.nstates, N).cpu().numpy()[:, rows].T
+        assert np.abs(yg - yr).max() <= TOL64 * np.abs(yr).max()
