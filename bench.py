@@ -1,0 +1,296 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Lanczos stage: Lanczos iterations/s on the drop-in size system.
+
+Workload (one step = one Lanczos iteration = H.v + alpha reduction + residual update +
+beta reduction): the 3-state, 8-mode vibronic Hamiltonian with basis [20,16,12,10,8,8,6,6]
+(88,473,600 functions per state, 265,420,800 in total), quadratic expansion, seeded
+synthetic coefficients (numpy default_rng(1002); the reference ships no input for it).
+The headline value is the plain FP64 path; the same line carries the mixed-precision
+(FP32 vectors, FP64 recurrence) rate, their ratio, and H.v bandwidth for both.
+
+Every vector (2.1 GB FP64) is larger than the 126 MB L2, so no cache flush is needed
+between steps.  Multi-GPU runs are replicas (the stage does not shard): each rank runs its
+own copy; value = total iterations/s over all ranks, timed as the max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --hv-only --precision mixed --steps 1 --warmup 1   (one H.v, for profiling)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Lanczos iter/s & H.v HBM GB/s: mixed vs FP64 at <=0.1 cm^-1; grad/fwd time"
+CONFIG_NUMBER = 2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both")
+    ap.add_argument("--hv-only", action="store_true", help="run H.v launches only (profiling)")
+    ap.add_argument("--config", type=int, default=CONFIG_NUMBER)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.stop = threading.Event()
+        self.th = None
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.th = threading.Thread(target=self._run, daemon=True)
+        self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        if self.th:
+            self.th.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for n, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_for(kernel: str, precision: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "hv_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(f"{kernel}:{precision}")
+
+
+def make_inputs(cfgn: int, tmpdir: str):
+    from nadvibs_b200 import synth
+    cfg = synth.config(cfgn)
+    return cfg, synth.write_inputs(tmpdir, cfg)
+
+
+def run_ours(args, rank, world, dev):
+    import torch
+    from nadvibs_b200 import _lib as L
+
+    torch.cuda.set_device(dev)
+    tmp = tempfile.mkdtemp(prefix=f"nvb_bench_{rank}_")
+    cfg, (basis, nadvibs) = make_inputs(args.config, tmp)
+    N = cfg.dimen * cfg.nstates
+    results = {}
+    precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+
+    def barrier():
+        if dist:
+            tdist.barrier()
+
+    def maxall(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        return t.item()
+
+    for prec in precs:
+        pflag = L.NVB_FP64 if prec == "fp64" else L.NVB_MIXED
+        eb = 8 if prec == "fp64" else 4
+        h = L.Handle.from_files(basis, nadvibs, device=dev, precision=pflag)
+        st = torch.cuda.Stream(device=dev)
+        h.set_stream(st.cuda_stream)
+        if args.hv_only:
+            dt = torch.float64 if prec == "fp64" else torch.float32
+            x = torch.randn(N, device=f"cuda:{dev}", dtype=dt)
+            y = torch.empty_like(x)
+            torch.cuda.synchronize()
+            with torch.cuda.stream(st):
+                for _ in range(args.warmup + args.steps):
+                    h.hv_ptr(x.data_ptr(), y.data_ptr(), L.DTYPE_F64 if prec == "fp64" else L.DTYPE_F32)
+            torch.cuda.synchronize()
+            h.close()
+            del x, y
+            torch.cuda.empty_cache()
+            continue
+        h.seed()
+        if args.warmup:
+            h.lanczos(args.warmup)
+        torch.cuda.synchronize()
+        barrier()
+        h.set_timing(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(dev) as clk:
+            e0.record(st)
+            a, b = h.lanczos(args.steps)
+            e1.record(st)
+            torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        ms_max = maxall(ms)
+        hv_ms, it_ms, n = h.timing()
+        results[prec] = dict(ms=ms_max, hv_ms_per=hv_ms / max(n, 1), it_ms_per=it_ms / max(n, 1),
+                             clocks=clk.summary(), bytes_hv=2 * N * eb, alpha=a[-3:].tolist(),
+                             beta=b[-3:].tolist(), launches=4 * args.steps)
+        h.close()
+        torch.cuda.empty_cache()
+    # end-to-end through the public API with host buffers: create from files (host input),
+    # seed, K iterations with alpha/beta returned to host memory, per iteration
+    e2e = None
+    if not args.hv_only:
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        h = L.Handle.from_files(basis, nadvibs, device=dev, precision=L.NVB_FP64)
+        h.seed()
+        a, b = h.lanczos(args.steps)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        h.close()
+        wall = maxall(t1 - t0)
+        h2d = os.path.getsize(basis) + os.path.getsize(nadvibs)
+        e2e = {"value": world * args.steps / wall, "unit": "iter/s",
+               "h2d_bytes_per_step": int(round(h2d / args.steps)), "d2h_bytes_per_step": 16}
+    return cfg, N, results, e2e
+
+
+def cpu_baseline_sample(cfgn: int, iters: int):
+    """The oracle's restatement of the reference (one streaming pass per term and shift,
+    Source/top.f90:672-818, and lanczos_step) on all host cores, bounded sample."""
+    from nadvibs_b200 import synth
+    from oracle import oracle as O
+    O.build()
+    cfg = synth.config(cfgn)
+    om, cc, pot = synth.draw(cfg)
+    S = O.system_from_arrays(cfg.basis, cfg.nstates, cfg.ordr, om, cc, pot)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    S.lanczos(iters, nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": iters / dt, "unit": "iter/s", "cores": cores, "kind": "port",
+            "sample": f"{iters} Lanczos iteration(s) of the {cfg.dimen * cfg.nstates:,}-element system "
+                      f"(seed + recurrence) by the C oracle, OpenMP on {cores} threads, {dt:.1f} s"}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        iters = max(1, min(args.steps, 3))
+        cb = cpu_baseline_sample(args.config, iters)
+        line = {"metric": METRIC, "value": cb["value"], "unit": "iter/s", "impl": "reference", "n_gpus": args.gpus,
+                "steps": iters, "warmup": 0, "ms_per_step": 1e3 / cb["value"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "config2: 3 states, basis [20,16,12,10,8,8,6,6], 265,420,800 functions, "
+                                       "ordr 2, plain Lanczos", "precision": "fp64", "cache": "inputs larger than L2"},
+                "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "iter/s", "h2d_bytes_per_step": 0,
+                                            "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    cfg, N, res, e2e = run_ours(args, rank, world, local)
+    if args.hv_only:
+        if rank == 0:
+            print(json.dumps({"hv_only": True, "launches": args.warmup + args.steps}))
+        return 0
+    peak, peak_kind = peaks()
+    main_prec = "fp64" if "fp64" in res else "mixed"
+    r = res[main_prec]
+    value = world * args.steps / (r["ms"] / 1e3)
+    hv_gbs = r["bytes_hv"] / (r["hv_ms_per"] / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if main_prec == "fp64" else "f32+f64",
+        "data": "synthetic (seeded basis.in/nadvibs.in, numpy default_rng(1002))",
+        "config": {"workload": "config2: 3 states, 8 modes, basis [20,16,12,10,8,8,6,6], 265,420,800 functions, "
+                               "ordr 2, plain Lanczos (reorthog=0)", "precision": main_prec,
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "cache": "inputs larger than L2 (2.1 GB FP64 vectors), no flush"},
+        "roofline": {"bound": "hbm", "achieved": hv_gbs, "peak": peak, "unit": "GB/s", "frac": hv_gbs / peak,
+                     "traffic": traffic_for("hv_slab", main_prec), "kernel": "H.v (k_hv_slab)",
+                     "algorithmic_bytes": r["bytes_hv"], "peak_kind": peak_kind},
+        "clocks": r["clocks"], "gpu_launches": r["launches"], "e2e": e2e,
+    }
+    if "mixed" in res and "fp64" in res:
+        m = res["mixed"]
+        mixed_rate = world * args.steps / (m["ms"] / 1e3)
+        line["mixed"] = {"value": mixed_rate, "unit": "iter/s", "ratio_vs_fp64": mixed_rate / value,
+                         "hv_ms": m["hv_ms_per"], "hv_gbs": m["bytes_hv"] / (m["hv_ms_per"] / 1e3) / 1e9,
+                         "hv_frac": m["bytes_hv"] / (m["hv_ms_per"] / 1e3) / 1e9 / peak}
+        line["fp64_hv_ms"] = r["hv_ms_per"]
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(args.config, 1)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as tdist
+        tdist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -151,6 +151,13 @@ int nvb_write_header(nvb_handle *h, const char *path);
 int nvb_lanczos_vectors(nvb_handle *h, void **cur, double *scur, void **prev, double *sprev, void **res,
                         double *sres);
 
+/* Per-phase device timing of nvb_lanczos (the reference writes per-phase wall times to
+ * output.dat, Source/top.f90:663-667,814-817,834-841): when enabled, CUDA events on the
+ * handle's stream bracket the H.v launch and the whole iteration; nvb_get_timing returns
+ * the accumulated milliseconds and the number of timed iterations.  Enabling resets them. */
+int nvb_set_timing(nvb_handle *h, int64_t enable);
+int nvb_get_timing(nvb_handle *h, double *hv_ms, double *iter_ms, int64_t *n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -62,6 +62,8 @@ _SIGS = {
     "nvb_write_eigenvalues": [C.c_void_p, C.c_char_p],
     "nvb_write_header": [C.c_void_p, C.c_char_p],
     "nvb_lanczos_vectors": [C.c_void_p] + [C.c_void_p] * 6,
+    "nvb_set_timing": [C.c_void_p, C.c_int64],
+    "nvb_get_timing": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
 }
 
 
@@ -225,3 +227,11 @@ class Handle:
         check(lib().nvb_lanczos_vectors(self.ptr, C.byref(p[0]), C.byref(s[0]), C.byref(p[1]), C.byref(s[1]),
                                         C.byref(p[2]), C.byref(s[2])))
         return [(p[i].value, s[i].value) for i in range(3)]
+
+    def set_timing(self, enable: bool = True):
+        check(lib().nvb_set_timing(self.ptr, int(enable)))
+
+    def timing(self):
+        a, b, n = C.c_double(), C.c_double(), C.c_int64()
+        check(lib().nvb_get_timing(self.ptr, C.byref(a), C.byref(b), C.byref(n)))
+        return a.value, b.value, n.value

@@ -115,6 +115,12 @@ static void create_common(nvb_handle *h, const nvb_params &p, const double *omeg
     h->precision = (int)h->opt.precision;
     plan_build(h->plan, h->sys, (int)h->opt.quirk_cubic, (int)h->opt.quirk_lower);
     plan_upload(h->plan);
+    if (h->opt.hv_kernel != 1) {
+        for (int i = 0; i < 2; ++i)
+            if (slab_build(h->slab[i], h->plan, h->sys, (int)h->opt.quirk_cubic, i == 0 ? 8 : 4)) slab_upload(h->slab[i]);
+        if (h->opt.hv_kernel == 2 && !h->slab[0].ok && !h->slab[1].ok)
+            fail(NVB_ERR_ARG, "slab kernel requested but the system does not suit it");
+    }
     h->reorthog = p.reorthog;
     h->chkorthog = p.chkorthog > 0 ? p.chkorthog : 100;
     h->rng_state = (uint64_t)h->opt.seed * 6364136223846793005ull + 1442695040888963407ull;
@@ -168,6 +174,8 @@ int nvb_destroy(nvb_handle *h) {
             if (h->stream) cudaStreamSynchronize(h->stream);
             lanczos_free(h);
             plan_free(h->plan);
+            slab_free(h->slab[0]);
+            slab_free(h->slab[1]);
             if (h->own_stream) cudaStreamDestroy(h->own_stream);
         }
     });
@@ -327,6 +335,24 @@ int nvb_lanczos_vectors(nvb_handle *h, void **cur, double *scur, void **prev, do
         if (sprev) *sprev = sc[h->prev];
         if (res) *res = h->buf[h->work];
         if (sres) *sres = sc[h->work];
+    });
+}
+
+int nvb_set_timing(nvb_handle *h, int64_t enable) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        h->timing = enable != 0;
+        h->t_hv_ms = h->t_iter_ms = 0.0;
+        h->n_timed = 0;
+    });
+}
+
+int nvb_get_timing(nvb_handle *h, double *hv_ms, double *iter_ms, int64_t *n) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        if (hv_ms) *hv_ms = h->t_hv_ms;
+        if (iter_ms) *iter_ms = h->t_iter_ms;
+        if (n) *n = h->n_timed;
     });
 }
 

@@ -6,11 +6,13 @@
 #include <vector>
 
 #include "plan.h"
+#include "slab.h"
 
 struct nvb_handle {
     nvb::System sys;
     nvb_options opt{};
     nvb::Plan plan;
+    nvb::SlabPlan slab[2];  // slab-tiled H.v plans for FP64 (0) and FP32 (1) vectors
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
@@ -37,6 +39,11 @@ struct nvb_handle {
     bool firststep = true;
     std::vector<std::pair<int64_t, int64_t>> orth_ranges;
     uint64_t rng_state = 0;
+    // per-phase device timing (CUDA events on the handle's stream)
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;  // 3 per iteration of a chunk: start, after H.v, end
+    double t_hv_ms = 0.0, t_iter_ms = 0.0;
+    int64_t n_timed = 0;
     // cached scratch for ad-hoc vectors
     void *tmp = nullptr;
     size_t tmp_bytes = 0;
@@ -54,6 +61,7 @@ void lanczos_run(nvb_handle *h, int64_t niter);
 void hv_any(nvb_handle *h, const void *x, void *y, int dtype, const double *scale_dev, double *alpha_part,
             int *nblocks_out);
 void ensure_partials(nvb_handle *h, int64_t n);
+void check_kernel_flags(nvb_handle *h);
 double device_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, int dtype);
 void *scratch_vector(nvb_handle *h, size_t bytes);
 }  // namespace nvb

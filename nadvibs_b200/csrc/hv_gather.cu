@@ -70,11 +70,12 @@ __global__ void __launch_bounds__(256) k_hv_gather(KArgs<T> A, const T *__restri
 #pragma unroll
             for (int b = 0; b < S; ++b) D[a][b] = A.cst[a * S + b];
         for (int i = 0; i < A.ndiag; ++i) {
-            const DevDiag dg = A.diag[i];
+            const DevDiag *dg = A.diag + i;
             T d1 = 1;
-            for (int l = 0; l < dg.nm; ++l) d1 = d1 * s_etab[dg.etab[l] + dig[dg.mode[l] * blockDim.x]];
-            const unsigned long long m0 = A.mask[2 * dg.term], m1 = A.mask[2 * dg.term + 1];
-            const T *cf = A.coef + (size_t)dg.term * S * S;
+            const int nm = dg->nm, term = dg->term;
+            for (int l = 0; l < nm; ++l) d1 = d1 * s_etab[dg->etab[l] + dig[dg->mode[l] * blockDim.x]];
+            const unsigned long long m0 = A.mask[2 * term], m1 = A.mask[2 * term + 1];
+            const T *cf = A.coef + (size_t)term * S * S;
 #pragma unroll
             for (int a = 0; a < S; ++a)
 #pragma unroll
@@ -92,19 +93,22 @@ __global__ void __launch_bounds__(256) k_hv_gather(KArgs<T> A, const T *__restri
                 if (b != a && A.dpair[a * S + b]) acc[a] = acc[a] + D[a][b] * xc[b];
         }
         for (int i = 0; i < A.nsteps; ++i) {
-            const DevStep st = A.steps[i];
+            const DevStep *st = A.steps + i;
             T e = 1;
             bool ok = true;
-            for (int l = 0; l < st.nm; ++l) {
-                const int n = dig[st.mode[l] * blockDim.x];
-                const int nc = n + st.sig[l];
-                if (nc < 0 || nc >= A.nfunc[st.mode[l]]) { ok = false; break; }
-                e = e * s_etab[st.etab[l] + (nc < n ? nc : n)];
+            const int nm = st->nm;
+            for (int l = 0; l < nm; ++l) {
+                const int md = st->mode[l];
+                const int n = dig[md * blockDim.x];
+                const int nc = n + st->sig[l];
+                if (nc < 0 || nc >= A.nfunc[md]) { ok = false; break; }
+                e = e * s_etab[st->etab[l] + (nc < n ? nc : n)];
             }
             if (!ok) continue;
-            const unsigned long long m0 = A.mask[2 * st.term], m1 = A.mask[2 * st.term + 1];
-            const T *cf = A.coef + (size_t)st.term * S * S;
-            const T *xs = x + r + st.stride;
+            const int term = st->term;
+            const unsigned long long m0 = A.mask[2 * term], m1 = A.mask[2 * term + 1];
+            const T *cf = A.coef + (size_t)term * S * S;
+            const T *xs = x + r + st->stride;
             T xb[S];
 #pragma unroll
             for (int b = 0; b < S; ++b) {

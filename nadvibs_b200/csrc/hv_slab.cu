@@ -1,0 +1,436 @@
+// Slab-tiled H.v (see slab.h for the decomposition).  One CTA per tile of T_F rows (fixed
+// slow digits), SLAB_RPT rows per thread.  For every slow-shift group the neighbour tile is
+// staged in shared memory by TMA bulk copies (cp.async.bulk, one per source state) that
+// complete on an mbarrier; two buffers alternate so the copy of group g+1 overlaps the
+// arithmetic of group g.  Fast shifts read the staged tile at row + stride; a zero halo of
+// `pad` elements on both sides and element factors that vanish outside the basis make
+// out-of-range fast shifts contribute exactly zero.  Slow element factors are uniform over
+// the CTA.  Accumulation is per row in registers; the epilogue scales, stores y and the
+// per-block partial of <scale*x, y>.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "slab.h"
+
+namespace nvb {
+
+template <typename T>
+struct SlabArgs {
+    const SlabStep *steps;
+    const SlabGroup *groups;
+    int ngroups;
+    int nstaged;
+    const SlabDiag *diag;
+    int ndiag;
+    const T *ftab;
+    int ftab_len;
+    const T *etab;
+    int etab_len;
+    const T *coef;                   // [nterms][S][S]
+    const unsigned long long *mask;  // [nterms][2]
+    const T *cst;                    // [S][S]
+    const int *dpair;                // [S][S]
+    const long long *slow_tshft;
+    const int *slow_nfunc;
+    const T *slow_omega;
+    const long long *fast_shft;
+    const T *fast_omega;
+    int m, nF, pad;
+    long long TF, dimen;
+    long long sstate;  // elements per state in a buffer: pad + TF + pad + tail
+    int *err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bounded wait on an mbarrier phase: returns false after ~2^22 polls (the copy never landed).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
+    const uint32_t a = smem_u32(bar);
+    for (int i = 0; i < (1 << 22); ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(phase)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ bool mbit(unsigned long long m0, unsigned long long m1, int bit) {
+    return bit < 64 ? ((m0 >> bit) & 1ull) : ((m1 >> (bit - 64)) & 1ull);
+}
+
+template <typename T>
+struct SlabMaxThreads { static constexpr int value = sizeof(T) == 8 ? 384 : 512; };
+
+template <typename T, int S>
+__global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T> A, const T *__restrict__ x, T *__restrict__ y,
+                                                 const double *__restrict__ scale_dev,
+                                                 double *__restrict__ alpha_part) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);  // SLAB_NBUF barriers
+    T *s_ftab = reinterpret_cast<T *>(smem + 64);
+    T *s_etab = s_ftab + A.ftab_len;
+    int *s_sd = reinterpret_cast<int *>(s_etab + A.etab_len);
+    size_t off = 64 + (size_t)(A.ftab_len + A.etab_len) * sizeof(T) + A.m * sizeof(int) + 16;
+    off = (off + 127) / 128 * 128;
+    T *s_buf = reinterpret_cast<T *>(smem + off);
+    const long long stride_state = A.sstate;  // per state in a buffer
+    const long long stride_buf = stride_state * S;
+
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const long long tile = blockIdx.x;
+    for (int i = tid; i < A.ftab_len; i += nth) s_ftab[i] = A.ftab[i];
+    for (int i = tid; i < A.etab_len; i += nth) s_etab[i] = A.etab[i];
+    if (tid == 0) {
+        long long rem = tile;
+        for (int l = 0; l < A.m; ++l) {
+            const long long d = rem / A.slow_tshft[l];
+            rem -= d * A.slow_tshft[l];
+            s_sd[l] = (int)d;
+        }
+        for (int b = 0; b < SLAB_NBUF; ++b) mbar_init(&bar[b], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // zero halos (never written by the copies)
+    for (int b = 0; b < SLAB_NBUF; ++b)
+        for (int s = 0; s < S; ++s) {
+            T *base = s_buf + b * stride_buf + s * stride_state;
+            for (int i = tid; i < A.pad; i += nth) base[i] = (T)0;
+            for (long long i = A.pad + A.TF + tid; i < stride_state; i += nth) base[i] = (T)0;
+        }
+    __syncthreads();
+
+    auto group_valid = [&](int g) {
+        const SlabGroup *G = A.groups + g;
+        for (int l = 0; l < A.m; ++l) {
+            const int n = s_sd[l] + G->sig[l];
+            if (n < 0 || n >= A.slow_nfunc[l]) return false;
+        }
+        return true;
+    };
+    auto next_valid = [&](int g) {
+        for (int q = g + 1; q < A.nstaged; ++q)
+            if (group_valid(q)) return q;
+        return -1;
+    };
+    const unsigned tile_bytes = (unsigned)(A.TF * sizeof(T));
+    auto issue = [&](int g, int b) {  // thread 0 only
+        const SlabGroup *G = A.groups + g;
+        const unsigned msk = G->state_mask;
+        fence_proxy_async();
+        mbar_expect_tx(&bar[b], (unsigned)__popc(msk) * tile_bytes);
+        const long long src_tile = tile + G->tile_shift;
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            if (msk & (1u << s))
+                bulk_g2s(s_buf + b * stride_buf + s * stride_state + A.pad, x + s * A.dimen + src_tile * A.TF, tile_bytes,
+                         &bar[b]);
+    };
+
+    // per-row fast digits (8 bits per fast mode)
+    uint32_t pk[SLAB_RPT];
+#pragma unroll
+    for (int k = 0; k < SLAB_RPT; ++k) {
+        const long long r = (long long)k * nth + tid;
+        uint32_t p = 0;
+        if (r < A.TF) {
+            long long rem = r;
+            for (int j = 0; j < A.nF; ++j) {
+                const long long d = rem / A.fast_shft[j];
+                rem -= d * A.fast_shft[j];
+                p |= (uint32_t)d << (8 * j);
+            }
+        }
+        pk[k] = p;
+    }
+    T acc[S][SLAB_RPT];
+    T xown[S][SLAB_RPT];
+#pragma unroll
+    for (int a = 0; a < S; ++a)
+#pragma unroll
+        for (int k = 0; k < SLAB_RPT; ++k) { acc[a][k] = 0; xown[a][k] = 0; }
+
+    unsigned phase_bits = 0;  // bit b = parity of the next completion of buffer b
+    int g = 0, bi = 0;
+    int nxt = next_valid(0);
+    if (tid == 0) {
+        issue(0, 0);
+        if (nxt >= 0) issue(nxt, 1);
+    }
+    // Pure slow-shift groups: y_a += sum_b C_ab x_b(neighbour tile), C uniform over the CTA.
+    // Their loads go straight to global memory and run while a staged tile is in flight.
+    int dnext = A.nstaged;
+    const int ndirect = A.ngroups - A.nstaged;
+    const int quota = A.nstaged > 0 ? (ndirect + A.nstaged - 1) / A.nstaged : ndirect;
+    auto do_direct = [&](int count) {
+        while (count > 0 && dnext < A.ngroups) {
+            const int q = dnext++;
+            if (!group_valid(q)) continue;
+            --count;
+            const SlabGroup *G = A.groups + q;
+            T C[S][S];
+#pragma unroll
+            for (int a = 0; a < S; ++a)
+#pragma unroll
+                for (int b = 0; b < S; ++b) C[a][b] = 0;
+            for (int i = G->step_begin; i < G->step_end; ++i) {
+                const SlabStep *st = A.steps + i;
+                T sf = 1;
+                const int nsl = st->nslow;
+                for (int qq = 0; qq < nsl; ++qq) {
+                    const int n = s_sd[st->slow_mode[qq]];
+                    const int nc = n + st->slow_sig[qq];
+                    sf = sf * s_etab[st->slow_etab[qq] + (nc < n ? nc : n)];
+                }
+                const int term = st->term;
+                const unsigned long long m0 = A.mask[2 * term], m1 = A.mask[2 * term + 1];
+                const T *cf = A.coef + (size_t)term * S * S;
+#pragma unroll
+                for (int a = 0; a < S; ++a)
+#pragma unroll
+                    for (int b = 0; b < S; ++b)
+                        if (mbit(m0, m1, a * S + b)) C[a][b] = C[a][b] + cf[a * S + b] * sf;
+            }
+            const long long base = (tile + G->tile_shift) * A.TF;
+            const unsigned smask = G->state_mask;
+#pragma unroll
+            for (int b = 0; b < S; ++b) {
+                if (!(smask & (1u << b))) continue;
+                T xb[SLAB_RPT];
+                const T *src = x + b * A.dimen + base + tid;
+#pragma unroll
+                for (int k = 0; k < SLAB_RPT; ++k)
+                    xb[k] = ((long long)k * nth + tid < A.TF) ? __ldcg(src + (long long)k * nth) : (T)0;
+#pragma unroll
+                for (int a = 0; a < S; ++a)
+                    if (C[a][b] != (T)0) {
+#pragma unroll
+                        for (int k = 0; k < SLAB_RPT; ++k) acc[a][k] = acc[a][k] + C[a][b] * xb[k];
+                    }
+            }
+        }
+    };
+
+    bool failed = false;
+    while (g >= 0) {
+        do_direct(quota);
+        if (!mbar_wait(&bar[bi], (phase_bits >> bi) & 1u)) {
+            failed = true;
+            break;
+        }
+        phase_bits ^= 1u << bi;
+        const T *buf = s_buf + bi * stride_buf + A.pad;
+        if (g == 0) {
+            // diagonal section: D(n) (constants + zero-shift even terms) and harmonic energy
+#pragma unroll
+            for (int a = 0; a < S; ++a)
+#pragma unroll
+                for (int k = 0; k < SLAB_RPT; ++k) {
+                    const long long r = (long long)k * nth + tid;
+                    xown[a][k] = r < A.TF ? buf[a * stride_state + r] : (T)0;
+                }
+            T ekin[SLAB_RPT];
+            {
+                T slow_ekin = 0;
+                for (int l = 0; l < A.m; ++l) slow_ekin += A.slow_omega[l] * ((T)s_sd[l] + (T)0.5);
+#pragma unroll
+                for (int k = 0; k < SLAB_RPT; ++k) {
+                    T e = slow_ekin;
+                    for (int j = 0; j < A.nF; ++j) e += A.fast_omega[j] * ((T)((pk[k] >> (8 * j)) & 0xFFu) + (T)0.5);
+                    ekin[k] = e;
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < S; ++a)
+#pragma unroll
+                for (int k = 0; k < SLAB_RPT; ++k) {
+                    T v = (A.cst[a * S + a] + ekin[k]) * xown[a][k];
+#pragma unroll
+                    for (int b = 0; b < S; ++b)
+                        if (b != a && A.dpair[a * S + b]) v = v + A.cst[a * S + b] * xown[b][k];
+                    acc[a][k] += v;
+                }
+            for (int i = 0; i < A.ndiag; ++i) {
+                const SlabDiag *dg = A.diag + i;
+                T sf = 1;
+                const int nsl = dg->nslow, nfa = dg->nfast;
+                for (int q = 0; q < nsl; ++q) sf = sf * s_etab[dg->slow_etab[q] + s_sd[dg->slow_mode[q]]];
+                T e[SLAB_RPT];
+#pragma unroll
+                for (int k = 0; k < SLAB_RPT; ++k) e[k] = sf;
+                for (int q = 0; q < nfa; ++q) {
+                    const int sh = 8 * dg->fast_field[q];
+                    const T *row = s_ftab + dg->fast_row[q];
+#pragma unroll
+                    for (int k = 0; k < SLAB_RPT; ++k) e[k] = e[k] * row[(int)((pk[k] >> sh) & 0xFFu)];
+                }
+                const int dterm = dg->term;
+                const unsigned long long m0 = A.mask[2 * dterm], m1 = A.mask[2 * dterm + 1];
+#pragma unroll
+                for (int a = 0; a < S; ++a)
+#pragma unroll
+                    for (int b = 0; b < S; ++b)
+                        if (mbit(m0, m1, a * S + b) && A.dpair[a * S + b]) {
+                            const T c = A.coef[(size_t)dterm * S * S + a * S + b];
+#pragma unroll
+                            for (int k = 0; k < SLAB_RPT; ++k) acc[a][k] = acc[a][k] + c * e[k] * xown[b][k];
+                        }
+            }
+        }
+        const int sbeg = A.groups[g].step_begin, send = A.groups[g].step_end;
+        for (int i = sbeg; i < send; ++i) {
+            const SlabStep *st = A.steps + i;
+            T sf = 1;
+            const int nsl = st->nslow, nfa = st->nfast;
+            for (int q = 0; q < nsl; ++q) {
+                const int n = s_sd[st->slow_mode[q]];
+                const int nc = n + st->slow_sig[q];
+                sf = sf * s_etab[st->slow_etab[q] + (nc < n ? nc : n)];
+            }
+            T e[SLAB_RPT];
+#pragma unroll
+            for (int k = 0; k < SLAB_RPT; ++k) e[k] = sf;
+            for (int q = 0; q < nfa; ++q) {
+                const int sh = 8 * st->fast_field[q];
+                const T *row = s_ftab + st->fast_row[q];
+#pragma unroll
+                for (int k = 0; k < SLAB_RPT; ++k) e[k] = e[k] * row[(int)((pk[k] >> sh) & 0xFFu)];
+            }
+            const int term = st->term;
+            const int sstride = st->stride;
+            const unsigned long long m0 = A.mask[2 * term], m1 = A.mask[2 * term + 1];
+            const T *cf = A.coef + (size_t)term * S * S;
+#pragma unroll
+            for (int b = 0; b < S; ++b) {
+                bool need = false;
+#pragma unroll
+                for (int a = 0; a < S; ++a) need |= mbit(m0, m1, a * S + b);
+                if (!need) continue;
+                T xb[SLAB_RPT];
+                const T *src = buf + b * stride_state + sstride + tid;
+#pragma unroll
+                for (int k = 0; k < SLAB_RPT; ++k) xb[k] = src[(long long)k * nth] * e[k];
+#pragma unroll
+                for (int a = 0; a < S; ++a)
+                    if (mbit(m0, m1, a * S + b)) {
+                        const T c = cf[a * S + b];
+#pragma unroll
+                        for (int k = 0; k < SLAB_RPT; ++k) acc[a][k] = acc[a][k] + c * xb[k];
+                    }
+            }
+        }
+        __syncthreads();  // every thread is done with buffer bi
+        const int n2 = nxt >= 0 ? next_valid(nxt) : -1;
+        if (tid == 0 && n2 >= 0) issue(n2, bi);
+        g = nxt;
+        nxt = n2;
+        bi ^= 1;
+    }
+    if (failed) {
+        if (tid == 0) atomicExch(A.err, 1);
+        return;
+    }
+    do_direct(A.ngroups);
+    const T sc = scale_dev ? (T)(*scale_dev) : (T)1;
+    double part = 0.0;
+#pragma unroll
+    for (int a = 0; a < S; ++a)
+#pragma unroll
+        for (int k = 0; k < SLAB_RPT; ++k) {
+            const long long r = (long long)k * nth + tid;
+            if (r < A.TF) {
+                const T v = acc[a][k] * sc;
+                y[a * A.dimen + tile * A.TF + r] = v;
+                part += ((double)xown[a][k] * (double)sc) * (double)v;
+            }
+        }
+    if (alpha_part) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        __shared__ double red[32];
+        if ((tid & 31) == 0) red[tid >> 5] = part;
+        __syncthreads();
+        if (tid < 32) {
+            double v = tid < (nth >> 5) ? red[tid] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (tid == 0) alpha_part[blockIdx.x] = v;
+        }
+    }
+}
+
+template <typename T>
+static SlabArgs<T> slab_args(const SlabPlan &sp, const Plan &pl);
+
+template <>
+SlabArgs<double> slab_args<double>(const SlabPlan &sp, const Plan &pl) {
+    return SlabArgs<double>{sp.d_steps,       sp.d_groups,    (int)sp.groups.size(), sp.nstaged, sp.d_diag,
+                            (int)sp.diag.size(), sp.d_ftab,   (int)sp.ftab.size(),   pl.d_etab,
+                            (int)pl.h_etab.size(), pl.d_coef, pl.d_mask,             pl.d_const,
+                            pl.d_dpair,       sp.d_slow_tshft, sp.d_slow_nfunc,      sp.d_slow_omega,
+                            sp.d_fast_shft,   sp.d_fast_omega, sp.m,                 sp.nF,
+                            sp.pad,           sp.TF,           pl.dimen,             sp.sstate,
+                            sp.d_err};
+}
+template <>
+SlabArgs<float> slab_args<float>(const SlabPlan &sp, const Plan &pl) {
+    return SlabArgs<float>{sp.d_steps,        sp.d_groups,     (int)sp.groups.size(), sp.nstaged, sp.d_diag,
+                           (int)sp.diag.size(), sp.d_ftab_f,   (int)sp.ftab.size(),   pl.d_etab_f,
+                           (int)pl.h_etab.size(), pl.d_coef_f, pl.d_mask,             pl.d_const_f,
+                           pl.d_dpair,        sp.d_slow_tshft, sp.d_slow_nfunc,       sp.d_slow_omega_f,
+                           sp.d_fast_shft,    sp.d_fast_omega_f, sp.m,                sp.nF,
+                           sp.pad,            sp.TF,           pl.dimen,              sp.sstate,
+                           sp.d_err};
+}
+
+template <typename T, int S>
+static void launch_slab_s(const SlabPlan &sp, const Plan &pl, const T *x, T *y, const double *sc, double *ap,
+                          cudaStream_t st) {
+    const size_t smem = sp.smem_bytes[sizeof(T) == 8 ? 0 : 1];
+    cudaFuncSetAttribute(k_hv_slab<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_hv_slab<T, S><<<(unsigned)sp.ntiles, sp.threads, smem, st>>>(slab_args<T>(sp, pl), x, y, sc, ap);
+}
+
+template <typename T>
+void slab_launch(const SlabPlan &sp, const Plan &pl, const T *x, T *y, const double *scale, double *alpha_part,
+                 cudaStream_t st) {
+    switch (pl.S) {
+    case 1: launch_slab_s<T, 1>(sp, pl, x, y, scale, alpha_part, st); break;
+    case 2: launch_slab_s<T, 2>(sp, pl, x, y, scale, alpha_part, st); break;
+    case 3: launch_slab_s<T, 3>(sp, pl, x, y, scale, alpha_part, st); break;
+    case 4: launch_slab_s<T, 4>(sp, pl, x, y, scale, alpha_part, st); break;
+    default: fail(NVB_ERR_ARG, "slab kernel supports up to 4 states");
+    }
+}
+
+template void slab_launch<double>(const SlabPlan &, const Plan &, const double *, double *, const double *, double *,
+                                  cudaStream_t);
+template void slab_launch<float>(const SlabPlan &, const Plan &, const float *, float *, const double *, double *,
+                                 cudaStream_t);
+
+}  // namespace nvb

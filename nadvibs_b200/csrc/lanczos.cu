@@ -139,12 +139,33 @@ void *scratch_vector(nvb_handle *h, size_t bytes) {
 void hv_any(nvb_handle *h, const void *x, void *y, int dtype, const double *scale_dev, double *alpha_part,
             int *nblocks_out) {
     if (alpha_part == nullptr && nblocks_out) *nblocks_out = 0;
+    const SlabPlan &sp = h->slab[dtype == NVB_DTYPE_F32 ? 1 : 0];
+    const bool aligned = ((uintptr_t)x % 16) == 0;
+    if (sp.ok && aligned && h->opt.hv_kernel != 1) {
+        if (dtype == NVB_DTYPE_F64)
+            slab_launch<double>(sp, h->plan, (const double *)x, (double *)y, scale_dev, alpha_part, h->stream);
+        else
+            slab_launch<float>(sp, h->plan, (const float *)x, (float *)y, scale_dev, alpha_part, h->stream);
+        CK(cudaGetLastError());
+        if (nblocks_out) *nblocks_out = (int)sp.ntiles;
+        return;
+    }
     if (dtype == NVB_DTYPE_F64)
         hv_gather_launch<double>(h->plan, (const double *)x, (double *)y, scale_dev, alpha_part, h->stream);
     else
         hv_gather_launch<float>(h->plan, (const float *)x, (float *)y, scale_dev, alpha_part, h->stream);
     CK(cudaGetLastError());
     if (nblocks_out) *nblocks_out = hv_gather_blocks(h->plan);
+}
+
+// A slab kernel whose tile copy never completed sets its error flag and stops early.
+void check_kernel_flags(nvb_handle *h) {
+    for (int i = 0; i < 2; ++i)
+        if (h->slab[i].ok && h->slab[i].d_err) {
+            int e = 0;
+            CK(cudaMemcpy(&e, h->slab[i].d_err, sizeof(int), cudaMemcpyDeviceToHost));
+            if (e) fail(NVB_ERR_CUDA, "slab H.v: a shared-memory tile copy did not complete (kernel gave up waiting)");
+        }
 }
 
 static void grow_scalars(nvb_handle *h, int64_t need) {
@@ -181,6 +202,8 @@ void lanczos_alloc(nvb_handle *h) {
 }
 
 void lanczos_free(nvb_handle *h) {
+    for (auto e : h->ev) cudaEventDestroy(e);
+    h->ev.clear();
     for (int i = 0; i < 3; ++i)
         if (h->buf[i]) { cudaFree(h->buf[i]); h->buf[i] = nullptr; }
     if (h->d_alpha) cudaFree(h->d_alpha);
@@ -271,16 +294,19 @@ static void passB_launch(nvb_handle *h, int64_t it, int *blocks) {
 }
 
 // One Lanczos iteration, stream-ordered, no host synchronisation.
-static void lanczos_iter(nvb_handle *h, int64_t it) {
+static void lanczos_iter(nvb_handle *h, int64_t it, int slot) {
     const int dt = h->precision == NVB_MIXED ? NVB_DTYPE_F32 : NVB_DTYPE_F64;
     int nb = 0;
+    if (h->timing) CK(cudaEventRecord(h->ev[3 * slot], h->stream));
     hv_any(h, h->buf[h->cur], h->buf[h->work], dt, h->d_scale + h->cur, h->d_part, &nb);
+    if (h->timing) CK(cudaEventRecord(h->ev[3 * slot + 1], h->stream));
     k_finalize<<<1, FIN_THREADS, 0, h->stream>>>(h->d_part, nb, h->d_alpha + it, 0, nullptr, h->d_status, (int)it);
     if (dt == NVB_DTYPE_F32) passB_launch<float>(h, it, &nb);
     else passB_launch<double>(h, it, &nb);
     k_finalize<<<1, FIN_THREADS, 0, h->stream>>>(h->d_part, nb, h->d_beta + it, 1, h->d_scale + h->work,
                                                  h->d_status, (int)it);
     CK(cudaGetLastError());
+    if (h->timing) CK(cudaEventRecord(h->ev[3 * slot + 2], h->stream));
     const int old_prev = h->prev;
     h->prev = h->cur;
     h->cur = h->work;
@@ -295,10 +321,25 @@ void lanczos_run(nvb_handle *h, int64_t niter) {
     int64_t done = 0;
     while (done < niter) {
         const int64_t n = std::min(chunk, niter - done);
-        for (int64_t k = 0; k < n; ++k) lanczos_iter(h, h->iters + done + k + 1);
+        if (h->timing && h->ev.size() < (size_t)(3 * chunk)) {
+            for (auto e : h->ev) cudaEventDestroy(e);
+            h->ev.assign(3 * chunk, nullptr);
+            for (auto &e : h->ev) CK(cudaEventCreate(&e));
+        }
+        for (int64_t k = 0; k < n; ++k) lanczos_iter(h, h->iters + done + k + 1, (int)k);
         int st[2] = {0, 0};
         CK(cudaMemcpyAsync(st, h->d_status, sizeof st, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
+        check_kernel_flags(h);
+        if (h->timing)
+            for (int64_t k = 0; k < n; ++k) {
+                float a = 0.f, b = 0.f;
+                CK(cudaEventElapsedTime(&a, h->ev[3 * k], h->ev[3 * k + 1]));
+                CK(cudaEventElapsedTime(&b, h->ev[3 * k], h->ev[3 * k + 2]));
+                h->t_hv_ms += a;
+                h->t_iter_ms += b;
+                h->n_timed += 1;
+            }
         done += n;
         if (st[0] != 0) {
             const int64_t total = h->iters + done;

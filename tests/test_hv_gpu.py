@@ -63,6 +63,32 @@ def test_hv_small_systems_fp64_and_fp32(seed, nstates, basis, ordr, quirks):
     assert np.abs(y32 - y_ref).max() <= TOL32 * scale
 
 
+MEDIUM = [(31, 1, [8, 8, 6, 6, 6, 4], 2), (32, 2, [8, 6, 8, 6, 6, 4], 3), (33, 3, [10, 8, 6, 4, 4, 4], 2),
+          (34, 4, [10, 8, 4, 4, 4, 4], 4), (35, 3, [12, 10, 8, 8, 6, 6], 2)]
+
+
+@pytest.mark.parametrize("seed,nstates,basis,ordr", MEDIUM)
+@pytest.mark.parametrize("quirks", [(1, 1), (0, 0)])
+def test_hv_slab_kernel_matches_oracle(seed, nstates, basis, ordr, quirks):
+    """Systems large enough for the slab-tiled kernel (hv_kernel=2 forces it; creation fails
+    if the system does not suit it), against the oracle and the gather kernel."""
+    cfg = synth.random_small(seed, nstates, basis, ordr)
+    om, cc, pot = synth.draw_small(cfg)
+    S = O.system_from_arrays(basis, nstates, ordr, om, cc, pot, quirk_cubic=bool(quirks[0]),
+                             quirk_lower=bool(quirks[1]))
+    x = np.random.default_rng(seed).normal(size=S.ntotal)
+    y_ref = S.hv(x, nthreads=8)
+    scale = np.abs(y_ref).max()
+    with _handle(_params(cfg), om, cc, pot, quirk_cubic=quirks[0], quirk_lower=quirks[1], hv_kernel=2) as h:
+        y64 = _hv_gpu(h, x)
+        y32 = _hv_gpu(h, x, torch.float32)
+    with _handle(_params(cfg), om, cc, pot, quirk_cubic=quirks[0], quirk_lower=quirks[1], hv_kernel=1) as hg:
+        g64 = _hv_gpu(hg, x)
+    assert np.abs(g64 - y_ref).max() <= TOL64 * scale
+    assert np.abs(y64 - y_ref).max() <= TOL64 * scale
+    assert np.abs(y32 - y_ref).max() <= TOL32 * scale
+
+
 @pytest.mark.parametrize("n", [1, 4])
 def test_hv_benchmark_systems_full(n):
     cfg = synth.config(n)
