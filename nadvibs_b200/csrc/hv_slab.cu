@@ -1,12 +1,18 @@
 // Slab-tiled H.v (see slab.h for the decomposition).  One CTA per tile of T_F rows (fixed
-// slow digits), SLAB_RPT rows per thread.  For every slow-shift group the neighbour tile is
-// staged in shared memory by TMA bulk copies (cp.async.bulk, one per source state) that
-// complete on an mbarrier; two buffers alternate so the copy of group g+1 overlaps the
-// arithmetic of group g.  Fast shifts read the staged tile at row + stride; a zero halo of
-// `pad` elements on both sides and element factors that vanish outside the basis make
-// out-of-range fast shifts contribute exactly zero.  Slow element factors are uniform over
-// the CTA.  Accumulation is per row in registers; the epilogue scales, stores y and the
-// per-block partial of <scale*x, y>.
+// slow digits), SLAB_RPT rows per thread.
+//
+// Prologue: the CTA folds, for every step, the slow element factors of its tile (uniform over
+// the CTA) into the S x S coupling block of the step's term and packs the step's fast part
+// (shift, fast table rows, state masks) into shared memory.
+// Staged groups (steps with fast shifts, and the own tile): the neighbour tile x(p + sigma_S)
+// is copied to shared memory by TMA bulk copies (cp.async.bulk, one per source state) that
+// complete on an mbarrier; two buffers alternate so the copy of the next staged group
+// overlaps the arithmetic of the current one.  Fast shifts read the staged tile at
+// row + stride; a zero halo and element factors that vanish outside the basis make
+// out-of-range fast shifts contribute exactly zero.
+// Direct groups (pure slow shifts): y_a += sum_b C_ab x_b(p + sigma_S) with C uniform; their
+// loads go straight to global memory while a staged copy is in flight.
+// Epilogue: scale, store y, and the per-block partial of <scale*x, y>.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -18,6 +24,7 @@ namespace nvb {
 template <typename T>
 struct SlabArgs {
     const SlabStep *steps;
+    int nsteps;
     const SlabGroup *groups;
     int ngroups;
     int nstaged;
@@ -42,9 +49,7 @@ struct SlabArgs {
     int *err;
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
@@ -80,27 +85,35 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-__device__ __forceinline__ bool mbit(unsigned long long m0, unsigned long long m1, int bit) {
-    return bit < 64 ? ((m0 >> bit) & 1ull) : ((m1 >> (bit - 64)) & 1ull);
-}
-
 template <typename T>
-struct SlabMaxThreads { static constexpr int value = sizeof(T) == 8 ? 384 : 512; };
+struct SlabMaxThreads {
+    static constexpr int value = sizeof(T) == 8 ? 384 : 512;
+};
+
+// packed step word: nfast (3 bits) | fast fields (4 x 2 bits) << 3 | column mask (4) << 11 |
+// pair mask (16) << 15
+__device__ __forceinline__ int info_nfast(unsigned w) { return (int)(w & 7u); }
+__device__ __forceinline__ int info_field(unsigned w, int q) { return (int)((w >> (3 + 2 * q)) & 3u); }
+__device__ __forceinline__ unsigned info_cols(unsigned w) { return (w >> 11) & 15u; }
+__device__ __forceinline__ unsigned info_pairs(unsigned w) { return w >> 15; }
 
 template <typename T, int S>
-__global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T> A, const T *__restrict__ x, T *__restrict__ y,
-                                                 const double *__restrict__ scale_dev,
-                                                 double *__restrict__ alpha_part) {
+__global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T> A, const T *__restrict__ x,
+                                                                      T *__restrict__ y,
+                                                                      const double *__restrict__ scale_dev,
+                                                                      double *__restrict__ alpha_part) {
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);  // SLAB_NBUF barriers
-    T *s_ftab = reinterpret_cast<T *>(smem + 64);
-    T *s_etab = s_ftab + A.ftab_len;
-    int *s_sd = reinterpret_cast<int *>(s_etab + A.etab_len);
-    size_t off = 64 + (size_t)(A.ftab_len + A.etab_len) * sizeof(T) + A.m * sizeof(int) + 16;
-    off = (off + 127) / 128 * 128;
-    T *s_buf = reinterpret_cast<T *>(smem + off);
-    const long long stride_state = A.sstate;  // per state in a buffer
+    const SlabLayout Lo = slab_layout(A.ftab_len, A.etab_len, A.nsteps, S, A.m, A.sstate, (int)sizeof(T));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+    T *s_ftab = reinterpret_cast<T *>(smem + Lo.ftab);
+    T *s_etab = reinterpret_cast<T *>(smem + Lo.etab);
+    T *s_cm = reinterpret_cast<T *>(smem + Lo.cm);
+    int4 *s_info = reinterpret_cast<int4 *>(smem + Lo.info);
+    int *s_sd = reinterpret_cast<int *>(smem + Lo.sd);
+    T *s_buf = reinterpret_cast<T *>(smem + Lo.buf);
+    const long long stride_state = A.sstate;
     const long long stride_buf = stride_state * S;
+    constexpr int S2 = S * S;
 
     const int tid = threadIdx.x, nth = blockDim.x;
     const long long tile = blockIdx.x;
@@ -116,7 +129,6 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
         for (int b = 0; b < SLAB_NBUF; ++b) mbar_init(&bar[b], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // zero halos (never written by the copies)
     for (int b = 0; b < SLAB_NBUF; ++b)
         for (int s = 0; s < S; ++s) {
             T *base = s_buf + b * stride_buf + s * stride_state;
@@ -124,6 +136,40 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
             for (long long i = A.pad + A.TF + tid; i < stride_state; i += nth) base[i] = (T)0;
         }
     __syncthreads();
+    // per-CTA step tables
+    for (int i = tid; i < A.nsteps; i += nth) {
+        const SlabStep *st = A.steps + i;
+        T sf = 1;
+        bool ok = true;
+        const int nsl = st->nslow;
+        for (int q = 0; q < nsl; ++q) {
+            const int md = st->slow_mode[q];
+            const int n = s_sd[md];
+            const int nc = n + st->slow_sig[q];
+            if (nc < 0 || nc >= A.slow_nfunc[md]) {
+                ok = false;
+                break;
+            }
+            sf = sf * s_etab[st->slow_etab[q] + (nc < n ? nc : n)];
+        }
+        const int term = st->term;
+        const unsigned pm = ok ? (unsigned)(A.mask[2 * term] & 0xFFFFull) : 0u;
+        unsigned cols = 0;
+#pragma unroll
+        for (int ab = 0; ab < S2; ++ab) {
+            const bool on = (pm >> ab) & 1u;
+            s_cm[i * S2 + ab] = on ? A.coef[(size_t)term * S2 + ab] * sf : (T)0;
+            if (on) cols |= 1u << (ab % S);
+        }
+        const int nfa = st->nfast;
+        unsigned w = (unsigned)nfa | (cols << 11) | (pm << 15);
+        int fr[4] = {0, 0, 0, 0};
+        for (int q = 0; q < nfa; ++q) {
+            w |= (unsigned)st->fast_field[q] << (3 + 2 * q);
+            fr[q] = st->fast_row[q];
+        }
+        s_info[i] = make_int4(st->stride, (int)w, fr[0] | (fr[1] << 16), fr[2] | (fr[3] << 16));
+    }
 
     auto group_valid = [&](int g) {
         const SlabGroup *G = A.groups + g;
@@ -148,8 +194,8 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
 #pragma unroll
         for (int s = 0; s < S; ++s)
             if (msk & (1u << s))
-                bulk_g2s(s_buf + b * stride_buf + s * stride_state + A.pad, x + s * A.dimen + src_tile * A.TF, tile_bytes,
-                         &bar[b]);
+                bulk_g2s(s_buf + b * stride_buf + s * stride_state + A.pad, x + s * A.dimen + src_tile * A.TF,
+                         tile_bytes, &bar[b]);
     };
 
     // per-row fast digits (8 bits per fast mode)
@@ -173,17 +219,20 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
 #pragma unroll
     for (int a = 0; a < S; ++a)
 #pragma unroll
-        for (int k = 0; k < SLAB_RPT; ++k) { acc[a][k] = 0; xown[a][k] = 0; }
+        for (int k = 0; k < SLAB_RPT; ++k) {
+            acc[a][k] = 0;
+            xown[a][k] = 0;
+        }
 
     unsigned phase_bits = 0;  // bit b = parity of the next completion of buffer b
     int g = 0, bi = 0;
     int nxt = next_valid(0);
+    __syncthreads();  // step tables complete
     if (tid == 0) {
         issue(0, 0);
         if (nxt >= 0) issue(nxt, 1);
     }
-    // Pure slow-shift groups: y_a += sum_b C_ab x_b(neighbour tile), C uniform over the CTA.
-    // Their loads go straight to global memory and run while a staged tile is in flight.
+
     int dnext = A.nstaged;
     const int ndirect = A.ngroups - A.nstaged;
     const int quota = A.nstaged > 0 ? (ndirect + A.nstaged - 1) / A.nstaged : ndirect;
@@ -193,29 +242,13 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
             if (!group_valid(q)) continue;
             --count;
             const SlabGroup *G = A.groups + q;
-            T C[S][S];
+            T C[S2];
 #pragma unroll
-            for (int a = 0; a < S; ++a)
+            for (int ab = 0; ab < S2; ++ab) C[ab] = 0;
+            const int sb = G->step_begin, se = G->step_end;
+            for (int i = sb; i < se; ++i)
 #pragma unroll
-                for (int b = 0; b < S; ++b) C[a][b] = 0;
-            for (int i = G->step_begin; i < G->step_end; ++i) {
-                const SlabStep *st = A.steps + i;
-                T sf = 1;
-                const int nsl = st->nslow;
-                for (int qq = 0; qq < nsl; ++qq) {
-                    const int n = s_sd[st->slow_mode[qq]];
-                    const int nc = n + st->slow_sig[qq];
-                    sf = sf * s_etab[st->slow_etab[qq] + (nc < n ? nc : n)];
-                }
-                const int term = st->term;
-                const unsigned long long m0 = A.mask[2 * term], m1 = A.mask[2 * term + 1];
-                const T *cf = A.coef + (size_t)term * S * S;
-#pragma unroll
-                for (int a = 0; a < S; ++a)
-#pragma unroll
-                    for (int b = 0; b < S; ++b)
-                        if (mbit(m0, m1, a * S + b)) C[a][b] = C[a][b] + cf[a * S + b] * sf;
-            }
+                for (int ab = 0; ab < S2; ++ab) C[ab] += s_cm[i * S2 + ab];
             const long long base = (tile + G->tile_shift) * A.TF;
             const unsigned smask = G->state_mask;
 #pragma unroll
@@ -228,9 +261,9 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
                     xb[k] = ((long long)k * nth + tid < A.TF) ? __ldcg(src + (long long)k * nth) : (T)0;
 #pragma unroll
                 for (int a = 0; a < S; ++a)
-                    if (C[a][b] != (T)0) {
+                    if (C[a * S + b] != (T)0) {
 #pragma unroll
-                        for (int k = 0; k < SLAB_RPT; ++k) acc[a][k] = acc[a][k] + C[a][b] * xb[k];
+                        for (int k = 0; k < SLAB_RPT; ++k) acc[a][k] = acc[a][k] + C[a * S + b] * xb[k];
                     }
             }
         }
@@ -246,7 +279,7 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
         phase_bits ^= 1u << bi;
         const T *buf = s_buf + bi * stride_buf + A.pad;
         if (g == 0) {
-            // diagonal section: D(n) (constants + zero-shift even terms) and harmonic energy
+            // diagonal section: harmonic energy, constants and zero-shift even terms
 #pragma unroll
             for (int a = 0; a < S; ++a)
 #pragma unroll
@@ -290,13 +323,13 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
                     for (int k = 0; k < SLAB_RPT; ++k) e[k] = e[k] * row[(int)((pk[k] >> sh) & 0xFFu)];
                 }
                 const int dterm = dg->term;
-                const unsigned long long m0 = A.mask[2 * dterm], m1 = A.mask[2 * dterm + 1];
+                const unsigned pm = (unsigned)(A.mask[2 * dterm] & 0xFFFFull);
 #pragma unroll
                 for (int a = 0; a < S; ++a)
 #pragma unroll
                     for (int b = 0; b < S; ++b)
-                        if (mbit(m0, m1, a * S + b) && A.dpair[a * S + b]) {
-                            const T c = A.coef[(size_t)dterm * S * S + a * S + b];
+                        if (((pm >> (a * S + b)) & 1u) && A.dpair[a * S + b]) {
+                            const T c = A.coef[(size_t)dterm * S2 + a * S + b];
 #pragma unroll
                             for (int k = 0; k < SLAB_RPT; ++k) acc[a][k] = acc[a][k] + c * e[k] * xown[b][k];
                         }
@@ -304,41 +337,47 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
         }
         const int sbeg = A.groups[g].step_begin, send = A.groups[g].step_end;
         for (int i = sbeg; i < send; ++i) {
-            const SlabStep *st = A.steps + i;
-            T sf = 1;
-            const int nsl = st->nslow, nfa = st->nfast;
-            for (int q = 0; q < nsl; ++q) {
-                const int n = s_sd[st->slow_mode[q]];
-                const int nc = n + st->slow_sig[q];
-                sf = sf * s_etab[st->slow_etab[q] + (nc < n ? nc : n)];
-            }
+            const int4 inf = s_info[i];
+            const unsigned w = (unsigned)inf.y;
+            const int nfa = info_nfast(w);
             T e[SLAB_RPT];
 #pragma unroll
-            for (int k = 0; k < SLAB_RPT; ++k) e[k] = sf;
-            for (int q = 0; q < nfa; ++q) {
-                const int sh = 8 * st->fast_field[q];
-                const T *row = s_ftab + st->fast_row[q];
+            for (int k = 0; k < SLAB_RPT; ++k) e[k] = 1;
+            if (nfa >= 1) {
+                const T *row = s_ftab + (inf.z & 0xFFFF);
+                const int sh = 8 * info_field(w, 0);
 #pragma unroll
-                for (int k = 0; k < SLAB_RPT; ++k) e[k] = e[k] * row[(int)((pk[k] >> sh) & 0xFFu)];
+                for (int k = 0; k < SLAB_RPT; ++k) e[k] = row[(int)((pk[k] >> sh) & 0xFFu)];
+                if (nfa >= 2) {
+                    const T *row2 = s_ftab + ((unsigned)inf.z >> 16);
+                    const int sh2 = 8 * info_field(w, 1);
+#pragma unroll
+                    for (int k = 0; k < SLAB_RPT; ++k) e[k] *= row2[(int)((pk[k] >> sh2) & 0xFFu)];
+                    for (int q = 2; q < nfa; ++q) {
+                        const T *rq = s_ftab + (q == 2 ? (inf.w & 0xFFFF) : ((unsigned)inf.w >> 16));
+                        const int shq = 8 * info_field(w, q);
+#pragma unroll
+                        for (int k = 0; k < SLAB_RPT; ++k) e[k] *= rq[(int)((pk[k] >> shq) & 0xFFu)];
+                    }
+                }
             }
-            const int term = st->term;
-            const int sstride = st->stride;
-            const unsigned long long m0 = A.mask[2 * term], m1 = A.mask[2 * term + 1];
-            const T *cf = A.coef + (size_t)term * S * S;
+            const unsigned cols = info_cols(w), pairs = info_pairs(w);
+            const T *cm = s_cm + i * S2;
 #pragma unroll
             for (int b = 0; b < S; ++b) {
-                bool need = false;
-#pragma unroll
-                for (int a = 0; a < S; ++a) need |= mbit(m0, m1, a * S + b);
-                if (!need) continue;
+                if (!((cols >> b) & 1u)) continue;
                 T xb[SLAB_RPT];
-                const T *src = buf + b * stride_state + sstride + tid;
+                const T *src = buf + b * stride_state + inf.x + tid;
 #pragma unroll
-                for (int k = 0; k < SLAB_RPT; ++k) xb[k] = src[(long long)k * nth] * e[k];
+                for (int k = 0; k < SLAB_RPT; ++k) xb[k] = src[(long long)k * nth];
+                if (nfa >= 1) {
+#pragma unroll
+                    for (int k = 0; k < SLAB_RPT; ++k) xb[k] *= e[k];
+                }
 #pragma unroll
                 for (int a = 0; a < S; ++a)
-                    if (mbit(m0, m1, a * S + b)) {
-                        const T c = cf[a * S + b];
+                    if ((pairs >> (a * S + b)) & 1u) {
+                        const T c = cm[a * S + b];
 #pragma unroll
                         for (int k = 0; k < SLAB_RPT; ++k) acc[a][k] = acc[a][k] + c * xb[k];
                     }
@@ -385,27 +424,45 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
 }
 
 template <typename T>
-static SlabArgs<T> slab_args(const SlabPlan &sp, const Plan &pl);
-
-template <>
-SlabArgs<double> slab_args<double>(const SlabPlan &sp, const Plan &pl) {
-    return SlabArgs<double>{sp.d_steps,       sp.d_groups,    (int)sp.groups.size(), sp.nstaged, sp.d_diag,
-                            (int)sp.diag.size(), sp.d_ftab,   (int)sp.ftab.size(),   pl.d_etab,
-                            (int)pl.h_etab.size(), pl.d_coef, pl.d_mask,             pl.d_const,
-                            pl.d_dpair,       sp.d_slow_tshft, sp.d_slow_nfunc,      sp.d_slow_omega,
-                            sp.d_fast_shft,   sp.d_fast_omega, sp.m,                 sp.nF,
-                            sp.pad,           sp.TF,           pl.dimen,             sp.sstate,
-                            sp.d_err};
-}
-template <>
-SlabArgs<float> slab_args<float>(const SlabPlan &sp, const Plan &pl) {
-    return SlabArgs<float>{sp.d_steps,        sp.d_groups,     (int)sp.groups.size(), sp.nstaged, sp.d_diag,
-                           (int)sp.diag.size(), sp.d_ftab_f,   (int)sp.ftab.size(),   pl.d_etab_f,
-                           (int)pl.h_etab.size(), pl.d_coef_f, pl.d_mask,             pl.d_const_f,
-                           pl.d_dpair,        sp.d_slow_tshft, sp.d_slow_nfunc,       sp.d_slow_omega_f,
-                           sp.d_fast_shft,    sp.d_fast_omega_f, sp.m,                sp.nF,
-                           sp.pad,            sp.TF,           pl.dimen,              sp.sstate,
-                           sp.d_err};
+static SlabArgs<T> slab_args(const SlabPlan &sp, const Plan &pl) {
+    SlabArgs<T> a{};
+    a.steps = sp.d_steps;
+    a.nsteps = (int)sp.steps.size();
+    a.groups = sp.d_groups;
+    a.ngroups = (int)sp.groups.size();
+    a.nstaged = sp.nstaged;
+    a.diag = sp.d_diag;
+    a.ndiag = (int)sp.diag.size();
+    a.ftab_len = (int)sp.ftab.size();
+    a.etab_len = (int)pl.h_etab.size();
+    a.mask = pl.d_mask;
+    a.dpair = pl.d_dpair;
+    a.slow_tshft = sp.d_slow_tshft;
+    a.slow_nfunc = sp.d_slow_nfunc;
+    a.fast_shft = sp.d_fast_shft;
+    a.m = sp.m;
+    a.nF = sp.nF;
+    a.pad = sp.pad;
+    a.TF = sp.TF;
+    a.dimen = pl.dimen;
+    a.sstate = sp.sstate;
+    a.err = sp.d_err;
+    if constexpr (sizeof(T) == 8) {
+        a.ftab = (const T *)sp.d_ftab;
+        a.etab = (const T *)pl.d_etab;
+        a.coef = (const T *)pl.d_coef;
+        a.cst = (const T *)pl.d_const;
+        a.slow_omega = (const T *)sp.d_slow_omega;
+        a.fast_omega = (const T *)sp.d_fast_omega;
+    } else {
+        a.ftab = (const T *)sp.d_ftab_f;
+        a.etab = (const T *)pl.d_etab_f;
+        a.coef = (const T *)pl.d_coef_f;
+        a.cst = (const T *)pl.d_const_f;
+        a.slow_omega = (const T *)sp.d_slow_omega_f;
+        a.fast_omega = (const T *)sp.d_fast_omega_f;
+    }
+    return a;
 }
 
 template <typename T, int S>

@@ -6,6 +6,8 @@
 // stages the neighbour tile x(p + sigma_S) (all states it needs) in shared memory with TMA
 // bulk copies and applies the group's steps, whose fast parts are shifts inside the tile.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <vector>
 
@@ -87,6 +89,32 @@ struct SlabPlan {
     int *d_err = nullptr;
     size_t smem_bytes[2] = {0, 0};  // per precision (0 = FP64, 1 = FP32)
 };
+
+// Dynamic shared-memory layout of the slab kernel (byte offsets), shared by host and device.
+struct SlabLayout {
+    size_t ftab, etab, cm, info, sd, buf, total;
+};
+__host__ __device__ inline SlabLayout slab_layout(long long ftab_len, long long etab_len, long long nsteps, int S,
+                                                  int m, long long sstate, int eb) {
+    SlabLayout L;
+    size_t off = 64;  // mbarriers
+    L.ftab = off;
+    off += (size_t)ftab_len * eb;
+    L.etab = off;
+    off += (size_t)etab_len * eb;
+    L.cm = off;
+    off += (size_t)nsteps * S * S * eb;
+    off = (off + 15) / 16 * 16;
+    L.info = off;
+    off += (size_t)nsteps * 16;
+    L.sd = off;
+    off += (size_t)m * 4 + 16;
+    off = (off + 127) / 128 * 128;
+    L.buf = off;
+    off += (size_t)SLAB_NBUF * S * sstate * eb;
+    L.total = off;
+    return L;
+}
 
 // Builds the slab plan; returns false (and leaves ok=false) when the system does not suit
 // it (too few tiles, misaligned tiles, too many states/modes).

@@ -22,13 +22,9 @@ static int slab_threads(long long TF) {
 }
 
 size_t slab_smem(const SlabPlan &sp, const Plan &pl, int eb) {
-    size_t off = 64;  // mbarriers
-    off += sp.ftab.size() * eb;
-    off += pl.h_etab.size() * eb;
-    off += sp.m * sizeof(int) + 16;
-    off = (off + 127) / 128 * 128;
-    off += (size_t)SLAB_NBUF * pl.S * sp.sstate * eb;
-    return off;
+    return slab_layout((long long)sp.ftab.size(), (long long)pl.h_etab.size(), (long long)sp.steps.size(), pl.S, sp.m,
+                       sp.sstate, eb)
+        .total;
 }
 
 bool slab_build(SlabPlan &sp, const Plan &pl, const System &sys, int quirk_cubic, int eb) {
@@ -208,6 +204,7 @@ bool slab_build(SlabPlan &sp, const Plan &pl, const System &sys, int quirk_cubic
     }
     sp.nfrows = (int)frow.size();
     if (sp.ftab.empty()) sp.ftab.assign(pl.nmax, 0.0);
+    if (sp.ftab.size() > 65535) return false;  // fast row offsets are packed in 16 bits
     sp.smem_bytes[0] = slab_smem(sp, pl, 8);
     sp.smem_bytes[1] = slab_smem(sp, pl, 4);
     if (sp.smem_bytes[eb == 8 ? 0 : 1] > 227 * 1024) return false;
