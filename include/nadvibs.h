@@ -151,6 +151,12 @@ int nvb_write_header(nvb_handle *h, const char *path);
 int nvb_lanczos_vectors(nvb_handle *h, void **cur, double *scur, void **prev, double *sprev, void **res,
                         double *sres);
 
+/* <sa*a, sb*b> over the handle's total vector length (dimen*nstates) of two device vectors of
+ * dtype, summed in FP64 in a fixed order (block partials in the handle's scratch, then one
+ * block); the result is returned in host memory (the call synchronises the stream).
+ * Replaces GA_DDOT on the Lanczos vectors (e.g. Source/top.f90:829,833). */
+int nvb_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, int64_t dtype, double *result);
+
 /* Per-phase device timing of nvb_lanczos (the reference writes per-phase wall times to
  * output.dat, Source/top.f90:663-667,814-817,834-841): when enabled, CUDA events on the
  * handle's stream bracket the H.v launch and the whole iteration; nvb_get_timing returns

@@ -63,6 +63,7 @@ _SIGS = {
     "nvb_write_header": [C.c_void_p, C.c_char_p],
     "nvb_lanczos_vectors": [C.c_void_p] + [C.c_void_p] * 6,
     "nvb_set_timing": [C.c_void_p, C.c_int64],
+    "nvb_dot": [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_int64, C.c_void_p],
     "nvb_get_timing": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
 }
 
@@ -235,3 +236,8 @@ class Handle:
         a, b, n = C.c_double(), C.c_double(), C.c_int64()
         check(lib().nvb_get_timing(self.ptr, C.byref(a), C.byref(b), C.byref(n)))
         return a.value, b.value, n.value
+
+    def dot_ptr(self, a_ptr: int, b_ptr: int, dtype: int, sa: float = 1.0, sb: float = 1.0) -> float:
+        r = C.c_double()
+        check(lib().nvb_dot(self.ptr, C.c_void_p(a_ptr), sa, C.c_void_p(b_ptr), sb, dtype, C.byref(r)))
+        return r.value

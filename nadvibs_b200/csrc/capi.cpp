@@ -356,4 +356,13 @@ int nvb_get_timing(nvb_handle *h, double *hv_ms, double *iter_ms, int64_t *n) {
     });
 }
 
+int nvb_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, int64_t dtype, double *result) {
+    return guarded([&] {
+        if (!h || !a || !b || !result) fail(NVB_ERR_ARG, "null argument");
+        if (dtype != NVB_DTYPE_F64 && dtype != NVB_DTYPE_F32) fail(NVB_ERR_ARG, "bad dtype");
+        ensure_device(h);
+        *result = device_dot(h, a, sa, b, sb, (int)dtype);
+    });
+}
+
 }  // extern "C"

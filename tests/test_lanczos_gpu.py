@@ -106,3 +106,16 @@ def test_mixed_precision_ritz_within_targets():
             assert i32 == pytest.approx(i64, rel=1e-4)
         else:
             assert abs(i32 - i64) <= 1e-7
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_device_dot_matches_numpy(dt):
+    cfg, h, S = _setup(4)
+    with h:
+        g = torch.Generator(device="cuda").manual_seed(5)
+        a = torch.randn(S.ntotal, generator=g, device="cuda", dtype=dt)
+        b = torch.randn(S.ntotal, generator=g, device="cuda", dtype=dt)
+        torch.cuda.synchronize()
+        d = h.dot_ptr(a.data_ptr(), b.data_ptr(), L.DTYPE_F64 if dt == torch.float64 else L.DTYPE_F32, 0.5, 2.0)
+        ref = float(np.dot(a.double().cpu().numpy(), b.double().cpu().numpy()))
+        assert d == pytest.approx(ref, rel=1e-12, abs=1e-9)
