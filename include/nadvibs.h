@@ -157,6 +157,20 @@ int nvb_lanczos_vectors(nvb_handle *h, void **cur, double *scur, void **prev, do
  * Replaces GA_DDOT on the Lanczos vectors (e.g. Source/top.f90:829,833). */
 int nvb_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, int64_t dtype, double *result);
 
+/* Allocation-free variant of nvb_dot (no counterpart in the reference).  For callers that
+ * cannot allocate device memory -- a host program whose GPU memory is owned by its own pool
+ * allocator, or a loop that must not call cudaMalloc/cudaFree because they may synchronise
+ * the device.  Computes <sa*a, sb*b> for n elements of dtype and writes it to the device
+ * double *result_dev, asynchronously on stream (a cudaStream_t, NULL = default stream).
+ * No handle and no allocation: the block partials live in a static device array of this
+ * library (4097 doubles, ~32 KiB per GPU that loads it, kept until exit), so n <= 2^32
+ * (larger n fails with NVB_ERR_ARG).  All calls share that array and each overwrites the
+ * partials it reads; calls that overlap on the GPU race, so order them (one stream or
+ * events).  The first call on each device looks up the array's address
+ * (cudaGetSymbolAddress, once per device) and should come before any stream capture. */
+int nvb_dot_noalloc(const void *a, double sa, const void *b, double sb, int64_t n, int64_t dtype, double *result_dev,
+                    void *stream);
+
 /* Per-phase device timing of nvb_lanczos (the reference writes per-phase wall times to
  * output.dat, Source/top.f90:663-667,814-817,834-841): when enabled, CUDA events on the
  * handle's stream bracket the H.v launch and the whole iteration; nvb_get_timing returns

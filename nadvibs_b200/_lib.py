@@ -64,6 +64,7 @@ _SIGS = {
     "nvb_lanczos_vectors": [C.c_void_p] + [C.c_void_p] * 6,
     "nvb_set_timing": [C.c_void_p, C.c_int64],
     "nvb_dot": [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_int64, C.c_void_p],
+    "nvb_dot_noalloc": [C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p],
     "nvb_get_timing": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
 }
 
@@ -94,6 +95,13 @@ def check(rc: int) -> None:
 
 def _p(a: np.ndarray | None):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def dot_noalloc(a_ptr: int, b_ptr: int, n: int, dtype: int, result_ptr: int, stream_ptr: int = 0,
+                sa: float = 1.0, sb: float = 1.0) -> None:
+    """nvb_dot_noalloc: <sa*a, sb*b> written to the device double at result_ptr (no allocation)."""
+    check(lib().nvb_dot_noalloc(C.c_void_p(a_ptr), sa, C.c_void_p(b_ptr), sb, n, dtype, C.c_void_p(result_ptr),
+                                C.c_void_p(stream_ptr) if stream_ptr else None))
 
 
 def default_params() -> Params:
