@@ -151,6 +151,28 @@ int nvb_write_header(nvb_handle *h, const char *path);
 int nvb_lanczos_vectors(nvb_handle *h, void **cur, double *scur, void **prev, double *sprev, void **res,
                         double *sres);
 
+/* Restart state (make_restart / load_restartinfo + restore, Source/top.f90:1007-1049,
+ * Source/secondary.f90:872-892, Source/top.f90:557-588): restart.log (text: iteration counts,
+ * alpha(1:n), beta(0:n), and omega(1,0:n), omega(2,0:n) when re-orthogonalising) and
+ * nadvibs.35.0 (q1 = v(n-1), q2 = v(n), q3 = the unnormalised residual, each as nstates
+ * records of dimen FP64 values) in dir (NULL = current directory).  nvb_load_restart
+ * resumes the handle at iteration n; as the reference, it renames restart.log to
+ * restart.log.old and deletes nadvibs.35.0 once loaded.  Restarting from an iteration
+ * before the last one (which needs the reference's disk archive) is rejected. */
+int nvb_save_restart(nvb_handle *h, const char *dir);
+int nvb_load_restart(nvb_handle *h, const char *dir);
+
+/* Ritz vectors of the lowest nroots roots of T_n (n = iterations done) and their lead basis
+ * functions (identify_roots, Source/top.f90:1124-1230): for root r and j < k, the j-th
+ * largest |psi|^2 entry: state[r*k+j] (1-based), index[r*k+j] (1-based row),
+ * c2[r*k+j] = |psi|^2, phase[r*k+j] = sign of psi; pct[r*nstates+s] = percent weight of state
+ * s.  Vectors come from the device archive when it holds every iteration (options
+ * archive_max), otherwise the recurrence is replayed from the seed with the stored
+ * alpha/beta (two-pass Lanczos).  rootinfo_path (optional) receives rootinfo.dat in the
+ * reference's format.  Any output array may be NULL. */
+int nvb_lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state, int64_t *index, double *c2,
+                          int64_t *phase, double *pct, const char *rootinfo_path);
+
 /* <sa*a, sb*b> over the handle's total vector length (dimen*nstates) of two device vectors of
  * dtype, summed in FP64 in a fixed order (block partials in the handle's scratch, then one
  * block); the result is returned in host memory (the call synchronises the stream).

@@ -63,6 +63,9 @@ _SIGS = {
     "nvb_write_header": [C.c_void_p, C.c_char_p],
     "nvb_lanczos_vectors": [C.c_void_p] + [C.c_void_p] * 6,
     "nvb_set_timing": [C.c_void_p, C.c_int64],
+    "nvb_save_restart": [C.c_void_p, C.c_char_p],
+    "nvb_load_restart": [C.c_void_p, C.c_char_p],
+    "nvb_lead_contributors": [C.c_void_p, C.c_int64, C.c_int64] + [C.c_void_p] * 6,
     "nvb_dot": [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_int64, C.c_void_p],
     "nvb_dot_noalloc": [C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p],
     "nvb_get_timing": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
@@ -249,3 +252,20 @@ class Handle:
         r = C.c_double()
         check(lib().nvb_dot(self.ptr, C.c_void_p(a_ptr), sa, C.c_void_p(b_ptr), sb, dtype, C.byref(r)))
         return r.value
+
+    def save_restart(self, directory: str):
+        check(lib().nvb_save_restart(self.ptr, directory.encode()))
+
+    def load_restart(self, directory: str):
+        check(lib().nvb_load_restart(self.ptr, directory.encode()))
+
+    def lead_contributors(self, nroots: int, k: int, rootinfo: str | None = None):
+        S = self.sizes()["nstates"]
+        st = np.zeros(max(nroots * k, 1), np.int64); ix = np.zeros(max(nroots * k, 1), np.int64)
+        c2 = np.zeros(max(nroots * k, 1)); ph = np.zeros(max(nroots * k, 1), np.int64)
+        pct = np.zeros(nroots * S)
+        check(lib().nvb_lead_contributors(self.ptr, nroots, k, _p(st), _p(ix), _p(c2), _p(ph), _p(pct),
+                                          rootinfo.encode() if rootinfo else None))
+        n = nroots * k
+        return dict(state=st[:n].reshape(nroots, k), index=ix[:n].reshape(nroots, k),
+                    c2=c2[:n].reshape(nroots, k), phase=ph[:n].reshape(nroots, k), pct=pct.reshape(nroots, S))

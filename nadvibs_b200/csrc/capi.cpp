@@ -365,4 +365,29 @@ int nvb_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, i
     });
 }
 
+int nvb_save_restart(nvb_handle *h, const char *dir) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        ensure_device(h);
+        save_restart(h, dir);
+    });
+}
+
+int nvb_load_restart(nvb_handle *h, const char *dir) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        ensure_device(h);
+        load_restart(h, dir);
+    });
+}
+
+int nvb_lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state, int64_t *index, double *c2,
+                          int64_t *phase, double *pct, const char *rootinfo_path) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        ensure_device(h);
+        lead_contributors(h, nroots, k, state, index, c2, phase, pct, rootinfo_path);
+    });
+}
+
 }  // extern "C"

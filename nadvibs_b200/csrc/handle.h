@@ -22,6 +22,7 @@ struct nvb_handle {
     int cur = 0, prev = 1, work = 2;
     int64_t iters = 0;      // completed iterations
     bool seeded = false;
+    std::vector<double> seed_w;  // weights the seed was built from (replayed for Ritz vectors)
     int64_t cap = 0;        // capacity of d_alpha / d_beta (iterations)
     double *d_alpha = nullptr;  // [cap+1], alpha(i) at index i
     double *d_beta = nullptr;   // [cap+1], beta(i) at index i
@@ -64,4 +65,11 @@ void ensure_partials(nvb_handle *h, int64_t n);
 void check_kernel_flags(nvb_handle *h);
 double device_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, int dtype);
 void *scratch_vector(nvb_handle *h, size_t bytes);
+void grow_scalars_public(nvb_handle *h, int64_t need);
+void archive_ensure(nvb_handle *h, int64_t need);
+void archive_push(nvb_handle *h, int64_t it);
+void save_restart(nvb_handle *h, const char *dir);
+void load_restart(nvb_handle *h, const char *dir);
+void lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state, int64_t *index, double *c2,
+                       int64_t *phase, double *pct, const char *rootinfo);
 }  // namespace nvb

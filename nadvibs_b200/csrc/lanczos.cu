@@ -188,6 +188,8 @@ static void grow_scalars(nvb_handle *h, int64_t need) {
     h->cap = nc;
 }
 
+void grow_scalars_public(nvb_handle *h, int64_t need) { grow_scalars(h, need); }
+
 void lanczos_alloc(nvb_handle *h) {
     const size_t bytes = (size_t)h->ntotal() * h->elem_size();
     for (int i = 0; i < 3; ++i) {
@@ -229,6 +231,7 @@ void lanczos_seed(nvb_handle *h, const double *weights) {
     if (!h->buf[0]) lanczos_alloc(h);
     std::vector<double> w(S);
     for (int s = 0; s < S; ++s) w[s] = weights ? weights[s] : h->sys.prm.weights[s];
+    h->seed_w = w;
     double wsum = 0.0;
     for (double v : w) wsum += v;
     if (wsum == 0.0) wsum = 1.0;
@@ -297,6 +300,7 @@ static void passB_launch(nvb_handle *h, int64_t it, int *blocks) {
 static void lanczos_iter(nvb_handle *h, int64_t it, int slot) {
     const int dt = h->precision == NVB_MIXED ? NVB_DTYPE_F32 : NVB_DTYPE_F64;
     int nb = 0;
+    archive_push(h, it);
     if (h->timing) CK(cudaEventRecord(h->ev[3 * slot], h->stream));
     hv_any(h, h->buf[h->cur], h->buf[h->work], dt, h->d_scale + h->cur, h->d_part, &nb);
     if (h->timing) CK(cudaEventRecord(h->ev[3 * slot + 1], h->stream));
@@ -317,6 +321,7 @@ void lanczos_run(nvb_handle *h, int64_t niter) {
     if (!h->seeded) fail(NVB_ERR_STATE, "nvb_lanczos called before nvb_seed / nvb_load_restart");
     if (niter < 0) fail(NVB_ERR_ARG, "niter < 0");
     grow_scalars(h, h->iters + niter + 1);
+    archive_ensure(h, h->iters + niter);
     const int64_t chunk = 64;
     int64_t done = 0;
     while (done < niter) {
