@@ -133,6 +133,14 @@ int nvb_seed(nvb_handle *h, const double *weights);
  * ALL iterations done so far (iters = previous + niter); either may be NULL. */
 int nvb_lanczos(nvb_handle *h, int64_t niter, double *alpha, double *beta);
 
+/* Re-orthogonalisation mode as in basis.in (Source/secondary.f90:847-848): reorthog 0 none,
+ * 1 omega recurrence with exact checks every chkorthog iterations, 2 exact overlaps;
+ * partial re-orthogonalisation (set_omega + partial_orthog, Source/top.f90:844-1005) runs after
+ * every iteration from the second.  It needs every Lanczos vector in the device archive
+ * (options archive_max >= total iterations), else nvb_lanczos fails with NVB_ERR_ARG.  The
+ * omega recurrence's random draws use the options' seed (the reference is unseeded). */
+int nvb_set_reorthog(nvb_handle *h, int64_t reorthog, int64_t chkorthog);
+
 /* Ritz system of T_n, n <= iters (compute_ritzsystem, Source/secondary.f90:240-257):
  * E[n] ascending (hartree), bji[n] = |beta(n) s(n,i)|, inten[n] = s(1,i)^2, sign[n] of
  * s(1,i); vect (optional, n*n column-major) the eigenvectors of T_n. */

@@ -64,6 +64,7 @@ _SIGS = {
     "nvb_lanczos_vectors": [C.c_void_p] + [C.c_void_p] * 6,
     "nvb_set_timing": [C.c_void_p, C.c_int64],
     "nvb_save_restart": [C.c_void_p, C.c_char_p],
+    "nvb_set_reorthog": [C.c_void_p, C.c_int64, C.c_int64],
     "nvb_load_restart": [C.c_void_p, C.c_char_p],
     "nvb_lead_contributors": [C.c_void_p, C.c_int64, C.c_int64] + [C.c_void_p] * 6,
     "nvb_dot": [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_int64, C.c_void_p],
@@ -269,3 +270,6 @@ class Handle:
         n = nroots * k
         return dict(state=st[:n].reshape(nroots, k), index=ix[:n].reshape(nroots, k),
                     c2=c2[:n].reshape(nroots, k), phase=ph[:n].reshape(nroots, k), pct=pct.reshape(nroots, S))
+
+    def set_reorthog(self, reorthog: int, chkorthog: int = 100):
+        check(lib().nvb_set_reorthog(self.ptr, reorthog, chkorthog))

@@ -390,4 +390,13 @@ int nvb_lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *sta
     });
 }
 
+int nvb_set_reorthog(nvb_handle *h, int64_t reorthog, int64_t chkorthog) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        if (reorthog < 0 || chkorthog < 1) fail(NVB_ERR_ARG, "reorthog >= 0 and chkorthog >= 1 required");
+        h->reorthog = reorthog;
+        h->chkorthog = chkorthog;
+    });
+}
+
 }  // extern "C"

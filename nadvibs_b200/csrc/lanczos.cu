@@ -317,11 +317,59 @@ static void lanczos_iter(nvb_handle *h, int64_t it, int slot) {
     h->work = old_prev;
 }
 
+void reorth_after_iter(nvb_handle *h, int64_t it, int64_t niter_total);
+void reorth_init(nvb_handle *h, int64_t niter_total);
+
+// Iteration-by-iteration path of nvb_lanczos with re-orthogonalisation (set_omega +
+// partial_orthog after every iteration from the second, Source/main.f90:66-69).
+static void reorth_run(nvb_handle *h, int64_t niter) {
+    const int64_t total = h->iters + niter;
+    if (h->iters == 0) reorth_init(h, total);
+    if (h->timing && h->ev.size() < 3) {
+        for (auto e : h->ev) cudaEventDestroy(e);
+        h->ev.assign(3, nullptr);
+        for (auto &e : h->ev) CK(cudaEventCreate(&e));
+    }
+    for (int64_t k = 0; k < niter; ++k) {
+        const int64_t it = h->iters + 1;
+        lanczos_iter(h, it, 0);
+        int st[2] = {0, 0};
+        CK(cudaMemcpyAsync(st, h->d_status, sizeof st, cudaMemcpyDeviceToHost, h->stream));
+        double ab[2];
+        CK(cudaMemcpyAsync(&ab[0], h->d_alpha + it, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(&ab[1], h->d_beta + it, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        check_kernel_flags(h);
+        if (h->timing) {
+            float a = 0.f, b = 0.f;
+            CK(cudaEventElapsedTime(&a, h->ev[0], h->ev[1]));
+            CK(cudaEventElapsedTime(&b, h->ev[0], h->ev[2]));
+            h->t_hv_ms += a;
+            h->t_iter_ms += b;
+            h->n_timed += 1;
+        }
+        h->alpha.resize(it + 1);
+        h->beta.resize(it + 1);
+        h->alpha[it] = ab[0];
+        h->beta[it] = ab[1];
+        if (st[0] != 0) fail(NVB_ERR_BREAKDOWN, "Lanczos breakdown at iteration " + std::to_string(st[1]));
+        h->iters = it;
+        if (it > 1) reorth_after_iter(h, it, total);
+    }
+}
+
 void lanczos_run(nvb_handle *h, int64_t niter) {
     if (!h->seeded) fail(NVB_ERR_STATE, "nvb_lanczos called before nvb_seed / nvb_load_restart");
     if (niter < 0) fail(NVB_ERR_ARG, "niter < 0");
     grow_scalars(h, h->iters + niter + 1);
     archive_ensure(h, h->iters + niter);
+    if (h->reorthog > 0) {
+        if (h->opt.archive_max < h->iters + niter)
+            fail(NVB_ERR_ARG, "re-orthogonalisation needs every Lanczos vector: set archive_max >= " +
+                                  std::to_string(h->iters + niter) + " (the archive lives in device memory)");
+        reorth_run(h, niter);
+        return;
+    }
     const int64_t chunk = 64;
     int64_t done = 0;
     while (done < niter) {

@@ -119,3 +119,42 @@ def test_device_dot_matches_numpy(dt):
         d = h.dot_ptr(a.data_ptr(), b.data_ptr(), L.DTYPE_F64 if dt == torch.float64 else L.DTYPE_F32, 0.5, 2.0)
         ref = float(np.dot(a.double().cpu().numpy(), b.double().cpu().numpy()))
         assert d == pytest.approx(ref, rel=1e-12, abs=1e-9)
+
+
+@pytest.mark.parametrize("reorthog", [1, 2])
+def test_reorthogonalisation_removes_ghosts(reorthog):
+    """Partial re-orthogonalisation (reorthog 1 and 2) keeps the basis orthogonal to ~sqrt(eps):
+    converged roots appear once (no ghost copies) and match the oracle's exact-overlap run."""
+    from oracle import reorth
+    niter = 250
+    cfg, h, S = _setup(1, archive_max=niter)
+    with h:
+        h.set_reorthog(reorthog, 50)
+        h.seed()
+        a, b = h.lanczos(niter)
+        E, bji, inten, _, _ = h.ritz(niter)
+    conv = E[bji < 1e-8]
+    gaps = np.diff(np.sort(conv)) * O.AU2WAVE
+    assert len(conv) > 20
+    assert gaps.min() > 1e-3, "a converged root appears twice (ghost)"
+    ao, bo, V = reorth.lanczos_reorth_exact(S, 120)
+    Eo, bjio, _, _, _ = O.ritz(ao, bo[:121])
+    for e in Eo[bjio < 1e-10]:
+        assert np.min(np.abs(E - e)) * O.AU2WAVE < 1e-6
+    # plain Lanczos on the same system does produce ghosts by 250 iterations
+    cfg, hp, _ = _setup(1)
+    with hp:
+        hp.seed()
+        hp.lanczos(niter)
+        Ep, bjip, _, _, _ = hp.ritz(niter)
+    assert np.diff(np.sort(Ep[bjip < 1e-8])).min() * O.AU2WAVE < 1e-3
+
+
+def test_reorthogonalisation_needs_archive():
+    cfg, h, S = _setup(1)
+    with h:
+        h.set_reorthog(2, 100)
+        h.seed()
+        with pytest.raises(L.NvbError) as e:
+            h.lanczos(10)
+        assert e.value.code == -1
