@@ -161,14 +161,15 @@ int nvb_lanczos_vectors(nvb_handle *h, void **cur, double *scur, void **prev, do
 
 /* Restart state (make_restart / load_restartinfo + restore, Source/top.f90:1007-1049,
  * Source/secondary.f90:872-892, Source/top.f90:557-588): restart.log (text: iteration counts,
- * alpha(1:n), beta(0:n), and omega(1,0:n), omega(2,0:n) when re-orthogonalising) and
- * nadvibs.35.0 (q1 = v(n-1), q2 = v(n), q3 = the unnormalised residual, each as nstates
- * records of dimen FP64 values) in dir (NULL = current directory).  nvb_load_restart
- * resumes the handle at iteration n; as the reference, it renames restart.log to
- * restart.log.old and deletes nadvibs.35.0 once loaded.  Restarting from an iteration
- * before the last one (which needs the reference's disk archive) is rejected. */
-int nvb_save_restart(nvb_handle *h, const char *dir);
-int nvb_load_restart(nvb_handle *h, const char *dir);
+ * alpha(1:n), beta(0:n), and omega(1,0:n), omega(2,0:n) when re-orthogonalising) in dir
+ * (NULL = current directory, where the reference keeps it) and nadvibs.35.0 (q1 = v(n-1),
+ * q2 = v(n), q3 = the unnormalised residual, each as nstates records of dimen FP64 values) in
+ * vecdir (the reference's -o scratch directory; NULL = dir).  nvb_load_restart resumes the
+ * handle at iteration n; as the reference, it renames restart.log to restart.log.old and
+ * deletes nadvibs.35.0 once loaded.  Restarting from an iteration before the last one (which
+ * needs the reference's disk archive) is rejected. */
+int nvb_save_restart(nvb_handle *h, const char *dir, const char *vecdir);
+int nvb_load_restart(nvb_handle *h, const char *dir, const char *vecdir);
 
 /* Ritz vectors of the lowest nroots roots of T_n (n = iterations done) and their lead basis
  * functions (identify_roots, Source/top.f90:1124-1230): for root r and j < k, the j-th

@@ -63,9 +63,9 @@ _SIGS = {
     "nvb_write_header": [C.c_void_p, C.c_char_p],
     "nvb_lanczos_vectors": [C.c_void_p] + [C.c_void_p] * 6,
     "nvb_set_timing": [C.c_void_p, C.c_int64],
-    "nvb_save_restart": [C.c_void_p, C.c_char_p],
+    "nvb_save_restart": [C.c_void_p, C.c_char_p, C.c_char_p],
     "nvb_set_reorthog": [C.c_void_p, C.c_int64, C.c_int64],
-    "nvb_load_restart": [C.c_void_p, C.c_char_p],
+    "nvb_load_restart": [C.c_void_p, C.c_char_p, C.c_char_p],
     "nvb_lead_contributors": [C.c_void_p, C.c_int64, C.c_int64] + [C.c_void_p] * 6,
     "nvb_dot": [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_int64, C.c_void_p],
     "nvb_dot_noalloc": [C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p],
@@ -254,11 +254,11 @@ class Handle:
         check(lib().nvb_dot(self.ptr, C.c_void_p(a_ptr), sa, C.c_void_p(b_ptr), sb, dtype, C.byref(r)))
         return r.value
 
-    def save_restart(self, directory: str):
-        check(lib().nvb_save_restart(self.ptr, directory.encode()))
+    def save_restart(self, directory: str, vecdir: str | None = None):
+        check(lib().nvb_save_restart(self.ptr, directory.encode(), vecdir.encode() if vecdir else None))
 
-    def load_restart(self, directory: str):
-        check(lib().nvb_load_restart(self.ptr, directory.encode()))
+    def load_restart(self, directory: str, vecdir: str | None = None):
+        check(lib().nvb_load_restart(self.ptr, directory.encode(), vecdir.encode() if vecdir else None))
 
     def lead_contributors(self, nroots: int, k: int, rootinfo: str | None = None):
         S = self.sizes()["nstates"]

@@ -365,19 +365,19 @@ int nvb_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, i
     });
 }
 
-int nvb_save_restart(nvb_handle *h, const char *dir) {
+int nvb_save_restart(nvb_handle *h, const char *dir, const char *vecdir) {
     return guarded([&] {
         if (!h) fail(NVB_ERR_ARG, "null handle");
         ensure_device(h);
-        save_restart(h, dir);
+        save_restart(h, dir, vecdir);
     });
 }
 
-int nvb_load_restart(nvb_handle *h, const char *dir) {
+int nvb_load_restart(nvb_handle *h, const char *dir, const char *vecdir) {
     return guarded([&] {
         if (!h) fail(NVB_ERR_ARG, "null handle");
         ensure_device(h);
-        load_restart(h, dir);
+        load_restart(h, dir, vecdir);
     });
 }
 

@@ -68,8 +68,8 @@ void *scratch_vector(nvb_handle *h, size_t bytes);
 void grow_scalars_public(nvb_handle *h, int64_t need);
 void archive_ensure(nvb_handle *h, int64_t need);
 void archive_push(nvb_handle *h, int64_t it);
-void save_restart(nvb_handle *h, const char *dir);
-void load_restart(nvb_handle *h, const char *dir);
+void save_restart(nvb_handle *h, const char *dir, const char *vdir);
+void load_restart(nvb_handle *h, const char *dir, const char *vdir);
 void lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state, int64_t *index, double *c2,
                        int64_t *phase, double *pct, const char *rootinfo);
 }  // namespace nvb

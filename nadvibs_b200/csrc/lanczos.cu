@@ -367,6 +367,9 @@ void lanczos_run(nvb_handle *h, int64_t niter) {
         if (h->opt.archive_max < h->iters + niter)
             fail(NVB_ERR_ARG, "re-orthogonalisation needs every Lanczos vector: set archive_max >= " +
                                   std::to_string(h->iters + niter) + " (the archive lives in device memory)");
+        if (h->arch_n != h->iters)
+            fail(NVB_ERR_STATE, "re-orthogonalisation cannot resume from a restart: the earlier Lanczos vectors "
+                                "(the reference's disk archive) are not kept");
         reorth_run(h, niter);
         return;
     }

@@ -181,8 +181,9 @@ static void write_reals(FILE *f, const double *v, int64_t n) {
     if (n == 0) std::fprintf(f, "\n");
 }
 
-void save_restart(nvb_handle *h, const char *dir) {
+void save_restart(nvb_handle *h, const char *dir, const char *vdir) {
     if (!h->seeded || h->iters < 1) fail(NVB_ERR_STATE, "no Lanczos iterations to save");
+    if (!vdir) vdir = dir;
     const int64_t n = h->iters;
     const std::string rl = join(dir, "restart.log");
     FILE *f = std::fopen(rl.c_str(), "w");
@@ -207,7 +208,7 @@ void save_restart(nvb_handle *h, const char *dir) {
     double sc[3];
     CK(cudaMemcpyAsync(sc, h->d_scale, sizeof sc, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    const std::string vf = join(dir, "nadvibs.35.0");
+    const std::string vf = join(vdir, "nadvibs.35.0");
     FILE *g = std::fopen(vf.c_str(), "wb");
     if (!g) fail(NVB_ERR_IO, "cannot write " + vf);
     export_vector(h, h->buf[h->work], sc[h->work], g);
@@ -254,7 +255,8 @@ std::string read_file(const std::string &path);
 void lanczos_alloc(nvb_handle *h);
 void grow_scalars_public(nvb_handle *h, int64_t need);
 
-void load_restart(nvb_handle *h, const char *dir) {
+void load_restart(nvb_handle *h, const char *dir, const char *vdir) {
+    if (!vdir) vdir = dir;
     const std::string rl = join(dir, "restart.log");
     Tok t;
     {
@@ -285,7 +287,7 @@ void load_restart(nvb_handle *h, const char *dir) {
         o2 = t.vals(nload + 1);
     }
     if (!(b[nload] > 0.0)) fail(NVB_ERR_IO, "restart.log: beta(n) must be positive");
-    const std::string vf = join(dir, "nadvibs.35.0");
+    const std::string vf = join(vdir, "nadvibs.35.0");
     FILE *g = std::fopen(vf.c_str(), "rb");
     if (!g) fail(NVB_ERR_IO, "cannot open " + vf);
     if (!h->buf[0]) lanczos_alloc(h);
@@ -305,6 +307,7 @@ void load_restart(nvb_handle *h, const char *dir) {
     for (int64_t i = 0; i < nload; ++i) h->alpha[i + 1] = a[i];
     h->beta = b;
     h->iters = nload;
+    h->seed_w.assign(h->sys.prm.weights, h->sys.prm.weights + h->sys.S);
     h->omega1 = o1;
     h->omega2 = o2;
     h->seeded = true;
@@ -404,7 +407,9 @@ static void ritz_vectors(nvb_handle *h, int64_t nroots, const std::vector<double
         void *b3[3] = {nullptr, nullptr, nullptr};
         for (int i = 0; i < 3; ++i) CK(cudaMalloc(&b3[i], per));
         // seed: the same vector lanczos_seed builds
-        std::vector<double> w(h->seed_w);
+        // the seed's weights: those nvb_seed used, or basis.in's after a restart
+        std::vector<double> w(h->sys.prm.weights, h->sys.prm.weights + h->sys.S);
+        if ((int)h->seed_w.size() == h->sys.S) w = h->seed_w;
         double wsum = 0.0;
         for (double v : w) wsum += v;
         if (wsum == 0.0) wsum = 1.0;

@@ -1,0 +1,86 @@
+! ISO_C_BINDING interface to libnadvibs_gpu.so (include/nadvibs.h) for the NadVibS Fortran
+! driver.  The reference is built with -i8, so every integer here is integer(c_int64_t);
+! reals are real(c_double); strings must end with c_null_char.  Status codes: 0 ok, < 0 error
+! (nvb_last_error gives the message).
+module nadvibs_gpu
+  use iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: NVB_FP64 = 0, NVB_MIXED = 1
+
+  type, bind(C) :: nvb_options
+    integer(c_int64_t) :: precision, device, quirk_cubic, quirk_lower, archive_max, hv_kernel, seed
+  end type
+
+  interface
+    integer(c_int) function nvb_options_default(o) bind(C, name="nvb_options_default")
+      import :: c_int, nvb_options
+      type(nvb_options), intent(out) :: o
+    end function
+    integer(c_int) function nvb_create_from_files(basis, nadvibs, opt, h) bind(C, name="nvb_create_from_files")
+      import :: c_int, c_char, c_ptr, nvb_options
+      character(kind=c_char), dimension(*), intent(in) :: basis, nadvibs
+      type(nvb_options), intent(in) :: opt
+      type(c_ptr), intent(out) :: h
+    end function
+    integer(c_int) function nvb_destroy(h) bind(C, name="nvb_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    type(c_ptr) function nvb_last_error() bind(C, name="nvb_last_error")
+      import :: c_ptr
+    end function
+    integer(c_int) function nvb_set_reorthog(h, reorthog, chkorthog) bind(C, name="nvb_set_reorthog")
+      import :: c_int, c_int64_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: reorthog, chkorthog
+    end function
+    integer(c_int) function nvb_write_header(h, path) bind(C, name="nvb_write_header")
+      import :: c_int, c_char, c_ptr
+      type(c_ptr), value :: h
+      character(kind=c_char), dimension(*), intent(in) :: path
+    end function
+    integer(c_int) function nvb_seed(h, weights) bind(C, name="nvb_seed")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h, weights
+    end function
+    integer(c_int) function nvb_lanczos(h, niter, alpha, beta) bind(C, name="nvb_lanczos")
+      import :: c_int, c_int64_t, c_double, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: niter
+      real(c_double), dimension(*), intent(out) :: alpha, beta
+    end function
+    integer(c_int) function nvb_save_restart(h, dir, vecdir) bind(C, name="nvb_save_restart")
+      import :: c_int, c_char, c_ptr
+      type(c_ptr), value :: h
+      character(kind=c_char), dimension(*), intent(in) :: dir, vecdir
+    end function
+    integer(c_int) function nvb_load_restart(h, dir, vecdir) bind(C, name="nvb_load_restart")
+      import :: c_int, c_char, c_ptr
+      type(c_ptr), value :: h
+      character(kind=c_char), dimension(*), intent(in) :: dir, vecdir
+    end function
+    integer(c_int) function nvb_write_eigenvalues(h, path) bind(C, name="nvb_write_eigenvalues")
+      import :: c_int, c_char, c_ptr
+      type(c_ptr), value :: h
+      character(kind=c_char), dimension(*), intent(in) :: path
+    end function
+    integer(c_int) function nvb_ritz(h, n, e, bji, inten, sign, vect) bind(C, name="nvb_ritz")
+      import :: c_int, c_int64_t, c_double, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: n
+      real(c_double), dimension(*), intent(out) :: e, bji, inten
+      integer(c_int64_t), dimension(*), intent(out) :: sign
+      type(c_ptr), value :: vect
+    end function
+    integer(c_int) function nvb_lead_contributors(h, nroots, k, state, index, c2, phase, pct, rootinfo) &
+        bind(C, name="nvb_lead_contributors")
+      import :: c_int, c_int64_t, c_double, c_char, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: nroots, k
+      integer(c_int64_t), dimension(*), intent(out) :: state, index, phase
+      real(c_double), dimension(*), intent(out) :: c2, pct
+      character(kind=c_char), dimension(*), intent(in) :: rootinfo
+    end function
+  end interface
+end module nadvibs_gpu

@@ -252,3 +252,54 @@ def convolve_sigma(x, y, sigma, grid, aperture="Gaussian"):
         else:
             env[i] = np.sum(y * (1.0 / sigma / (1.0 + t * t)))
     return env / np.max(env)
+
+
+# ---------------------------------------------------------------- output.dat text
+def _I(v: int, w: int) -> str:
+    s = str(int(v))
+    return "*" * w if len(s) > w else s.rjust(w)
+
+
+def _F(v: float, w: int, d: int) -> str:
+    s = f"{v:.{d}f}"
+    return "*" * w if len(s) > w else s.rjust(w)
+
+
+def _ES(v: float, w: int, d: int) -> str:
+    m, e = f"{v:.{d}E}".split("E")
+    ex = int(e)
+    s = f"{m}E{ex:+03d}" if abs(ex) < 100 else f"{m}{ex:+04d}"
+    return "*" * w if len(s) > w else s.rjust(w)
+
+
+def eigen_table_lines(alpha, beta, omega, bjiconv: float):
+    """The text of compute_eigenvalues (Source/top.f90:1095-1112) from ZPVE to the last row."""
+    zpve, first, fac, rows = eigen_table(alpha, beta, omega, bjiconv)
+    out = [f"  ZPVE from nadvibs.in (reference state): {_F(zpve, 12, 4)} cm-1",
+           f"  FIRST eigenvalue:                       {_F(first, 12, 4)} cm-1",
+           f"  Intensity Factor (MAX Intensity):       {_F(fac, 12, 8)}",
+           "  Root  Index  Convergence     E(cm-1)        E(eV)     Intensity"]
+    for k, g, b, ecm, eev, it in rows:
+        out.append(_I(k, 6) + _I(g, 7) + _ES(b, 13, 4) + _F(ecm, 15, 5) + _F(eev, 12, 5) + _F(it, 12, 7))
+    return out
+
+
+def extract_spectrum(path: str, threshold: float = 1e-15):
+    """extract.py:22-50: (E_eV, I, convergence) rows of output.dat's table with convergence <
+    threshold and I != 0, in table order."""
+    with open(path) as f:
+        lines = f.readlines()
+    start = stop = None
+    for i, l in enumerate(lines):
+        if "Root  Index  Convergence     E(cm-1)        E(eV)     Intensity" in l:
+            start = i + 1
+        if "All requested eigenvalues computed." in l:
+            stop = i - 1
+            break
+    out = []
+    for l in lines[start:stop]:
+        t = l.split()
+        c, x, y = float(t[2]), float(t[4]), float(t[5])
+        if c < threshold and y != 0:
+            out.append((x, y, c))
+    return out
