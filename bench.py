@@ -130,22 +130,11 @@ def run_ours(args, rank, world, dev):
     tmp = tempfile.mkdtemp(prefix=f"nvb_bench_{rank}_")
     cfg, (basis, nadvibs) = make_inputs(args.config, tmp)
     N = cfg.dimen * cfg.nstates
+    from nadvibs_b200 import replicas
     results = {}
     precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
-    dist = world > 1
-    if dist:
-        import torch.distributed as tdist
-
-    def barrier():
-        if dist:
-            tdist.barrier()
-
-    def maxall(v):
-        if not dist:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        return t.item()
+    barrier = replicas.barrier
+    maxall = replicas.max_over_ranks
 
     for prec in precs:
         pflag = L.NVB_FP64 if prec == "fp64" else L.NVB_MIXED
@@ -246,11 +235,8 @@ def main():
         print(json.dumps(line))
         return 0
     if world > 1:
-        import torch
-        import torch.distributed as tdist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        from nadvibs_b200 import replicas
+        replicas.init("nccl", timeout_s=120)
     cfg, N, res, e2e = run_ours(args, rank, world, local)
     if args.hv_only:
         if rank == 0:
@@ -287,8 +273,8 @@ def main():
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
-        import torch.distributed as tdist
-        tdist.destroy_process_group()
+        from nadvibs_b200 import replicas
+        replicas.shutdown()
     return 0
 
 
