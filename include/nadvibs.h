@@ -182,6 +182,22 @@ int nvb_load_restart(nvb_handle *h, const char *dir, const char *vecdir);
 int nvb_lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state, int64_t *index, double *c2,
                           int64_t *phase, double *pct, const char *rootinfo_path);
 
+/* Adjoint contraction of the gradient path (no counterpart in the reference):
+ * grad[npot + nstblks + nmodes] = d<u|H(theta)|v>/d theta for theta = (the potterms of
+ * nvb_create's layout -- every nadvibs.in expansion coefficient, zero ones included --, the
+ * block constants concoef, the frequencies omega).  u, v are device vectors of dtype in the
+ * reference layout.  Couplings between different states are differentiated in their
+ * symmetric form (the lower-triangle-only constant coupling of the reference is a quirk of
+ * the forward product; see nvb_options.quirk_lower). */
+int nvb_hv_adjoint_coeffs(nvb_handle *h, const void *u, const void *v, int64_t dtype, double *grad);
+
+/* Hellmann-Feynman gradients of the lowest nroots Ritz energies of T_n (n = iterations
+ * done): grad[r*ncoef + i] = <psi_r|dH/dtheta_i|psi_r>/<psi_r|psi_r> with the Ritz vectors
+ * psi_r (archive or two-pass replay, as nvb_lead_contributors), ncoef = npot + nstblks +
+ * nmodes in the layout of nvb_hv_adjoint_coeffs; energies[nroots] (optional) the Ritz values.
+ * Exact derivatives for converged roots. */
+int nvb_hellmann_feynman(nvb_handle *h, int64_t nroots, double *grad, double *energies);
+
 /* <sa*a, sb*b> over the handle's total vector length (dimen*nstates) of two device vectors of
  * dtype, summed in FP64 in a fixed order (block partials in the handle's scratch, then one
  * block); the result is returned in host memory (the call synchronises the stream).

@@ -65,6 +65,8 @@ _SIGS = {
     "nvb_set_timing": [C.c_void_p, C.c_int64],
     "nvb_save_restart": [C.c_void_p, C.c_char_p, C.c_char_p],
     "nvb_set_reorthog": [C.c_void_p, C.c_int64, C.c_int64],
+    "nvb_hv_adjoint_coeffs": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p],
+    "nvb_hellmann_feynman": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
     "nvb_load_restart": [C.c_void_p, C.c_char_p, C.c_char_p],
     "nvb_lead_contributors": [C.c_void_p, C.c_int64, C.c_int64] + [C.c_void_p] * 6,
     "nvb_dot": [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_int64, C.c_void_p],
@@ -273,3 +275,19 @@ class Handle:
 
     def set_reorthog(self, reorthog: int, chkorthog: int = 100):
         check(lib().nvb_set_reorthog(self.ptr, reorthog, chkorthog))
+
+    def ncoef(self) -> int:
+        sz = self.sizes()
+        S = sz["nstates"]
+        return sz["npot"] + S * (S + 1) // 2 + sz["nmodes"]
+
+    def adjoint_ptr(self, u_ptr: int, v_ptr: int, dtype: int) -> np.ndarray:
+        g = np.zeros(self.ncoef())
+        check(lib().nvb_hv_adjoint_coeffs(self.ptr, C.c_void_p(u_ptr), C.c_void_p(v_ptr), dtype, _p(g)))
+        return g
+
+    def hellmann_feynman(self, nroots: int):
+        g = np.zeros((nroots, self.ncoef()))
+        e = np.zeros(nroots)
+        check(lib().nvb_hellmann_feynman(self.ptr, nroots, _p(g), _p(e)))
+        return e, g

@@ -1,0 +1,378 @@
+// Adjoint of H.v with respect to the Hamiltonian's input coefficients (no counterpart in the
+// reference, which has no derivative code).
+//
+// theta = (potterms in the nadvibs.in layout, concoef, omega).  With P_m[a][b] = <u_a|M_m|v_b>
+// for every monomial m of the file (zero coefficients included), C[a][b] = <u_a|v_b> and
+// K_k = sum_a <u_a|(n_k+1/2)|v_a>:
+//   d<u|H|v>/d c(block (i,j), m) = s_m (P_m[i][j] + [i!=j] P_m[j][i]),  s_m = prod omega^(-p/2)
+//   d<u|H|v>/d concoef(i,j)      = C[i][j] + [i!=j] C[j][i]
+//   d<u|H|v>/d omega_k           = K_k + sum_terms sum_pairs (-p_k/(2 omega_k)) coef_ab P_m[a][b]
+// M_m is the monomial's operator exactly as H.v applies it (analytic <m|x^p|n>, cubic quirk
+// per the handle's option); couplings between different states are taken symmetric.
+// One kernel pass per chunk of monomials: each thread walks rows (grid-stride) and keeps
+// TB*S*S FP64 accumulators; block partials are summed on the host in a fixed order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "handle.h"
+
+namespace nvb {
+
+#define CK(x)                                                                                    \
+    do {                                                                                         \
+        cudaError_t e_ = (x);                                                                    \
+        if (e_ != cudaSuccess) fail(NVB_ERR_CUDA, std::string(#x ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct AdjStep {  // one shift of one monomial
+    int mono;      // chunk-local monomial index
+    int nm;
+    int mode[MAX_ORDER];
+    int sig[MAX_ORDER];
+    int etab[MAX_ORDER];
+    long long stride;
+};
+
+constexpr int ADJ_THREADS = 256;
+
+template <typename T, int S, int TB>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adjoint(const AdjStep *__restrict__ steps, int nsteps,
+                                                        const double *__restrict__ etab, int etab_len,
+                                                        const int *__restrict__ nfunc,
+                                                        const long long *__restrict__ shft, int M, long long dimen,
+                                                        const T *__restrict__ u, const T *__restrict__ v,
+                                                        double *__restrict__ part) {
+    extern __shared__ double s_etab[];
+    for (int i = threadIdx.x; i < etab_len; i += blockDim.x) s_etab[i] = etab[i];
+    __syncthreads();
+    double acc[TB][S][S];
+#pragma unroll
+    for (int t = 0; t < TB; ++t)
+#pragma unroll
+        for (int a = 0; a < S; ++a)
+#pragma unroll
+            for (int b = 0; b < S; ++b) acc[t][a][b] = 0.0;
+    const long long gstride = (long long)gridDim.x * blockDim.x;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < dimen; r += gstride) {
+        int dig[64];
+        long long rem = r;
+        for (int k = 0; k < M; ++k) {
+            const long long d = rem / shft[k];
+            rem -= d * shft[k];
+            dig[k] = (int)d;
+        }
+        double ua[S];
+#pragma unroll
+        for (int a = 0; a < S; ++a) ua[a] = (double)u[a * dimen + r];
+        for (int i = 0; i < nsteps; ++i) {
+            const AdjStep *st = steps + i;
+            double e = 1.0;
+            bool ok = true;
+            const int nm = st->nm;
+            for (int l = 0; l < nm; ++l) {
+                const int md = st->mode[l];
+                const int n = dig[md], nc = n + st->sig[l];
+                if (nc < 0 || nc >= nfunc[md]) { ok = false; break; }
+                e *= s_etab[st->etab[l] + (nc < n ? nc : n)];
+            }
+            if (!ok) continue;
+            const long long c = r + st->stride;
+            double vb[S];
+#pragma unroll
+            for (int b = 0; b < S; ++b) vb[b] = (double)v[b * dimen + c] * e;
+            const int t = st->mono;
+#pragma unroll
+            for (int tt = 0; tt < TB; ++tt)
+                if (tt == t)
+#pragma unroll
+                    for (int a = 0; a < S; ++a)
+#pragma unroll
+                        for (int b = 0; b < S; ++b) acc[tt][a][b] += ua[a] * vb[b];
+        }
+    }
+    __shared__ double red[ADJ_THREADS];
+#pragma unroll
+    for (int t = 0; t < TB; ++t)
+#pragma unroll
+        for (int a = 0; a < S; ++a)
+#pragma unroll
+            for (int b = 0; b < S; ++b) {
+                red[threadIdx.x] = acc[t][a][b];
+                __syncthreads();
+                for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+                    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+                    __syncthreads();
+                }
+                if (threadIdx.x == 0) part[(long long)blockIdx.x * TB * S * S + (t * S + a) * S + b] = red[0];
+                __syncthreads();
+            }
+}
+
+// overlaps C[a][b] = <u_a|v_b> and harmonic K_k = sum_a <u_a|(n_k+1/2)|v_a>
+template <typename T, int S>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_diag(const long long *__restrict__ shft, int M, long long dimen,
+                                                         const T *__restrict__ u, const T *__restrict__ v,
+                                                         double *__restrict__ part) {
+    double c[S][S];
+    double kin[64];
+#pragma unroll
+    for (int a = 0; a < S; ++a)
+#pragma unroll
+        for (int b = 0; b < S; ++b) c[a][b] = 0.0;
+    for (int k = 0; k < M; ++k) kin[k] = 0.0;
+    const long long gstride = (long long)gridDim.x * blockDim.x;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < dimen; r += gstride) {
+        double ua[S], vb[S], uv = 0.0;
+#pragma unroll
+        for (int a = 0; a < S; ++a) {
+            ua[a] = (double)u[a * dimen + r];
+            vb[a] = (double)v[a * dimen + r];
+            uv += ua[a] * vb[a];
+        }
+#pragma unroll
+        for (int a = 0; a < S; ++a)
+#pragma unroll
+            for (int b = 0; b < S; ++b) c[a][b] += ua[a] * vb[b];
+        long long rem = r;
+        for (int k = 0; k < M; ++k) {
+            const long long d = rem / shft[k];
+            rem -= d * shft[k];
+            kin[k] += ((double)d + 0.5) * uv;
+        }
+    }
+    __shared__ double red[ADJ_THREADS];
+    const int nout = S * S + M;
+    for (int q = 0; q < nout; ++q) {
+        double val = 0.0;
+#pragma unroll
+        for (int a = 0; a < S; ++a)
+#pragma unroll
+            for (int b = 0; b < S; ++b)
+                if (q == a * S + b) val = c[a][b];
+        if (q >= S * S) val = kin[q - S * S];
+        red[threadIdx.x] = val;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[(long long)blockIdx.x * nout + q] = red[0];
+        __syncthreads();
+    }
+}
+
+static int smax_of(int p, int64_t nf) {
+    int s = p;
+    while (s > nf - 1) s -= 2;
+    return s;
+}
+
+struct Mono {
+    std::vector<int> modes, pows;
+};
+
+static std::vector<Mono> all_monomials(const System &sys) {
+    std::vector<Mono> out;
+    for (int d = 1; d <= sys.ordr; ++d)
+        for (auto &dig : monomials(sys.M, d)) {
+            Mono m;
+            for (int x : dig) {
+                auto it = std::find(m.modes.begin(), m.modes.end(), x - 1);
+                if (it == m.modes.end()) {
+                    m.modes.push_back(x - 1);
+                    m.pows.push_back(1);
+                } else m.pows[it - m.modes.begin()] += 1;
+            }
+            out.push_back(m);
+        }
+    return out;
+}
+
+template <typename T, int S, int TB>
+static void launch_chunk(nvb_handle *h, const std::vector<AdjStep> &steps, const T *u, const T *v, double *part,
+                         int grid) {
+    AdjStep *d = nullptr;
+    CK(cudaMalloc((void **)&d, std::max<size_t>(1, steps.size()) * sizeof(AdjStep)));
+    CK(cudaMemcpyAsync(d, steps.data(), steps.size() * sizeof(AdjStep), cudaMemcpyHostToDevice, h->stream));
+    const Plan &pl = h->plan;
+    k_adjoint<T, S, TB><<<grid, ADJ_THREADS, pl.h_etab.size() * sizeof(double), h->stream>>>(
+        d, (int)steps.size(), pl.d_etab, (int)pl.h_etab.size(), pl.d_nfunc, pl.d_shft, pl.M, pl.dimen, u, v, part);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    cudaFree(d);
+}
+
+template <typename T, int S>
+static void adjoint_s(nvb_handle *h, const T *u, const T *v, double *grad) {
+    constexpr int TB = S * S <= 4 ? 8 : (S * S <= 9 ? 3 : 2);
+    const System &sys = h->sys;
+    const Plan &pl = h->plan;
+    const int M = sys.M;
+    const auto monos = all_monomials(sys);
+    const int nm = (int)monos.size();
+    const int grid = 148 * 4;
+    // P[m][a][b]
+    std::vector<double> P((size_t)nm * S * S, 0.0);
+    double *part = nullptr;
+    CK(cudaMalloc((void **)&part, (size_t)grid * std::max(TB * S * S, S * S + M) * sizeof(double)));
+    for (int m0 = 0; m0 < nm; m0 += TB) {
+        std::vector<AdjStep> steps;
+        for (int t = m0; t < std::min(nm, m0 + TB); ++t) {
+            const Mono &mo = monos[t];
+            const int d = (int)mo.modes.size();
+            int sm[MAX_ORDER], sd[MAX_ORDER];
+            bool bad = false;
+            long long ns = 1;
+            for (int l = 0; l < d; ++l) {
+                sm[l] = smax_of(mo.pows[l], sys.nfunc[mo.modes[l]]);
+                if (sm[l] < 0) bad = true;
+                ns *= sm[l] + 1;
+                sd[l] = -sm[l];
+            }
+            if (bad) continue;
+            sd[d - 1] -= 2;
+            for (long long k = 0; k < ns; ++k) {
+                int l = d - 1;
+                while (sd[l] >= sm[l]) { sd[l] = -sm[l]; --l; }
+                sd[l] += 2;
+                AdjStep st{};
+                st.mono = t - m0;
+                st.nm = d;
+                long long stride = 0;
+                for (int q = 0; q < d; ++q) {
+                    st.mode[q] = mo.modes[q];
+                    st.sig[q] = sd[q];
+                    st.etab[q] = ((mo.pows[q] - 1) * ETAB_J + std::abs(sd[q])) * pl.nmax;
+                    stride += (long long)sd[q] * sys.shft[mo.modes[q]];
+                }
+                st.stride = stride;
+                steps.push_back(st);  // the zero shift of an all-even monomial included
+            }
+        }
+        launch_chunk<T, S, TB>(h, steps, u, v, part, grid);
+        std::vector<double> hp((size_t)grid * TB * S * S);
+        CK(cudaMemcpy(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int t = m0; t < std::min(nm, m0 + TB); ++t)
+            for (int ab = 0; ab < S * S; ++ab) {
+                double s = 0.0;
+                for (int g = 0; g < grid; ++g) s += hp[(size_t)g * TB * S * S + (t - m0) * S * S + ab];
+                P[(size_t)t * S * S + ab] = s;
+            }
+    }
+    // overlaps and harmonic part
+    k_adj_diag<T, S><<<grid, ADJ_THREADS, 0, h->stream>>>(pl.d_shft, M, pl.dimen, u, v, part);
+    CK(cudaGetLastError());
+    const int nout = S * S + M;
+    std::vector<double> hq((size_t)grid * nout);
+    CK(cudaMemcpyAsync(hq.data(), part, hq.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    cudaFree(part);
+    std::vector<double> Cq(nout, 0.0);
+    for (int q = 0; q < nout; ++q)
+        for (int g = 0; g < grid; ++g) Cq[q] += hq[(size_t)g * nout + q];
+    // assemble
+    const int nb = sys.nstblks();
+    const int64_t npot = (int64_t)sys.potterms.size();
+    std::vector<std::pair<int, int>> cp(nb);
+    for (int i = 1; i <= S; ++i)
+        for (int j = 1; j <= i; ++j) cp[i * (i - 1) / 2 + j - 1] = {i - 1, j - 1};
+    // monomial id of (order d, index k)
+    std::vector<int> mono_base(sys.ordr + 1, 0);
+    for (int d = 1; d <= sys.ordr; ++d) mono_base[d] = (d == 1 ? 0 : mono_base[d - 1] + (int)numut(M, d - 1));
+    std::vector<double> scale(nm, 1.0);
+    for (int t = 0; t < nm; ++t)
+        for (size_t l = 0; l < monos[t].modes.size(); ++l)
+            scale[t] /= std::sqrt(std::pow(sys.omega[monos[t].modes[l]], (double)monos[t].pows[l]));
+    for (int b = 0; b < nb; ++b) {
+        auto [i, j] = cp[b];
+        for (int d = 1; d <= sys.ordr; ++d) {
+            const int64_t off = sys.pot_offset[(size_t)b * sys.ordr + d - 1];
+            const int64_t cnt = numut(M, d);
+            for (int64_t k = 0; k < cnt; ++k) {
+                const int t = mono_base[d] + (int)k;
+                double g = P[(size_t)t * S * S + i * S + j];
+                if (i != j) g += P[(size_t)t * S * S + j * S + i];
+                grad[off + k] = scale[t] * g;
+            }
+        }
+        double gc = Cq[i * S + j];
+        if (i != j) gc += Cq[j * S + i];
+        grad[npot + b] = gc;
+    }
+    // frequencies: harmonic part plus the omega dependence of every scaled coefficient
+    for (int k = 0; k < M; ++k) grad[npot + nb + k] = Cq[S * S + k];
+    for (int b = 0; b < nb; ++b) {
+        auto [i, j] = cp[b];
+        for (int d = 1; d <= sys.ordr; ++d) {
+            const int64_t off = sys.pot_offset[(size_t)b * sys.ordr + d - 1];
+            const int64_t cnt = numut(M, d);
+            for (int64_t k = 0; k < cnt; ++k) {
+                const double c = sys.potterms[off + k];
+                if (c == 0.0) continue;
+                const int t = mono_base[d] + (int)k;
+                double g = P[(size_t)t * S * S + i * S + j];
+                if (i != j) g += P[(size_t)t * S * S + j * S + i];
+                for (size_t l = 0; l < monos[t].modes.size(); ++l) {
+                    const int md = monos[t].modes[l];
+                    grad[npot + nb + md] += -(double)monos[t].pows[l] / (2.0 * sys.omega[md]) * c * scale[t] * g;
+                }
+            }
+        }
+    }
+}
+
+void hv_adjoint(nvb_handle *h, const void *u, const void *v, int dtype, double *grad) {
+    const bool f32 = dtype == NVB_DTYPE_F32;
+#define ADJ_CASE(SS)                                                                  \
+    case SS:                                                                          \
+        if (f32) adjoint_s<float, SS>(h, (const float *)u, (const float *)v, grad);   \
+        else adjoint_s<double, SS>(h, (const double *)u, (const double *)v, grad);    \
+        break;
+    switch (h->sys.S) {
+        ADJ_CASE(1)
+        ADJ_CASE(2)
+        ADJ_CASE(3)
+        ADJ_CASE(4)
+    default: fail(NVB_ERR_ARG, "the adjoint supports up to 4 states");
+    }
+#undef ADJ_CASE
+}
+
+int64_t ncoef_of(const nvb_handle *h) { return (int64_t)h->sys.potterms.size() + h->sys.nstblks() + h->sys.M; }
+
+// Ritz vectors, declared in state.cu
+void ritz_vectors_public(nvb_handle *h, int64_t nroots, const std::vector<double> &V, double *psi);
+
+// Hellmann-Feynman: grad[r*ncoef + i] = <psi_r| dH/dtheta_i |psi_r> for the lowest nroots Ritz
+// vectors of T_n (normalised in FP64).
+void hellmann_feynman(nvb_handle *h, int64_t nroots, double *grad, double *energies) {
+    const int64_t n = h->iters;
+    if (n < 1) fail(NVB_ERR_STATE, "no Lanczos iterations");
+    if (nroots < 1 || nroots > n) fail(NVB_ERR_ARG, "nroots must be in 1..iterations");
+    const long long N = h->ntotal();
+    std::vector<double> E(n), V((size_t)n * n);
+    tridiag_eigen(n, h->alpha.data() + 1, h->beta.data() + 1, E.data(), V.data());
+    double *psi = nullptr;
+    CK(cudaMalloc((void **)&psi, (size_t)nroots * N * sizeof(double)));
+    try {
+        ritz_vectors_public(h, nroots, V, psi);
+        const int64_t nc = ncoef_of(h);
+        for (int64_t r = 0; r < nroots; ++r) {
+            double *p = psi + (size_t)r * N;
+            const double nrm2 = device_dot(h, p, 1.0, p, 1.0, NVB_DTYPE_F64);
+            hv_adjoint(h, p, p, NVB_DTYPE_F64, grad + r * nc);
+            for (int64_t i = 0; i < nc; ++i) grad[r * nc + i] /= nrm2;
+            if (energies) energies[r] = E[r];
+        }
+    } catch (...) {
+        cudaFree(psi);
+        throw;
+    }
+    cudaFree(psi);
+}
+
+}  // namespace nvb

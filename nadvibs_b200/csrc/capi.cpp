@@ -399,4 +399,21 @@ int nvb_set_reorthog(nvb_handle *h, int64_t reorthog, int64_t chkorthog) {
     });
 }
 
+int nvb_hv_adjoint_coeffs(nvb_handle *h, const void *u, const void *v, int64_t dtype, double *grad) {
+    return guarded([&] {
+        if (!h || !u || !v || !grad) fail(NVB_ERR_ARG, "null argument");
+        if (dtype != NVB_DTYPE_F64 && dtype != NVB_DTYPE_F32) fail(NVB_ERR_ARG, "bad dtype");
+        ensure_device(h);
+        hv_adjoint(h, u, v, (int)dtype, grad);
+    });
+}
+
+int nvb_hellmann_feynman(nvb_handle *h, int64_t nroots, double *grad, double *energies) {
+    return guarded([&] {
+        if (!h || !grad) fail(NVB_ERR_ARG, "null argument");
+        ensure_device(h);
+        hellmann_feynman(h, nroots, grad, energies);
+    });
+}
+
 }  // extern "C"

@@ -70,6 +70,9 @@ void archive_ensure(nvb_handle *h, int64_t need);
 void archive_push(nvb_handle *h, int64_t it);
 void save_restart(nvb_handle *h, const char *dir, const char *vdir);
 void load_restart(nvb_handle *h, const char *dir, const char *vdir);
+void hv_adjoint(nvb_handle *h, const void *u, const void *v, int dtype, double *grad);
+void hellmann_feynman(nvb_handle *h, int64_t nroots, double *grad, double *energies);
+int64_t ncoef_of(const nvb_handle *h);
 void lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state, int64_t *index, double *c2,
                        int64_t *phase, double *pct, const char *rootinfo);
 }  // namespace nvb

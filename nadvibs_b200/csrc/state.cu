@@ -474,6 +474,10 @@ static void ritz_vectors(nvb_handle *h, int64_t nroots, const std::vector<double
     cudaFree(dc);
 }
 
+void ritz_vectors_public(nvb_handle *h, int64_t nroots, const std::vector<double> &V, double *psi) {
+    ritz_vectors(h, nroots, V, psi);
+}
+
 void lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state, int64_t *index, double *c2,
                        int64_t *phase, double *pct, const char *rootinfo) {
     const int64_t n = h->iters;
