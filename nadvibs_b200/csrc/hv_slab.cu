@@ -43,7 +43,7 @@ struct SlabArgs {
     const T *slow_omega;
     const long long *fast_shft;
     const T *fast_omega;
-    int m, nF, pad;
+    int m, nF, pad, cols;
     long long TF, dimen;
     long long sstate;  // elements per state in a buffer: pad + TF + pad + tail
     int *err;
@@ -103,16 +103,19 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
                                                                       const double *__restrict__ scale_dev,
                                                                       double *__restrict__ alpha_part) {
     extern __shared__ __align__(128) unsigned char smem[];
-    const SlabLayout Lo = slab_layout(A.ftab_len, A.etab_len, A.nsteps, S, A.m, A.sstate, (int)sizeof(T));
+    const SlabLayout Lo =
+        slab_layout(A.ftab_len, A.etab_len, A.nsteps, A.ngroups - A.nstaged, S, A.m, A.sstate, (int)sizeof(T));
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
     T *s_ftab = reinterpret_cast<T *>(smem + Lo.ftab);
     T *s_etab = reinterpret_cast<T *>(smem + Lo.etab);
     T *s_cm = reinterpret_cast<T *>(smem + Lo.cm);
+    T *s_cg = reinterpret_cast<T *>(smem + Lo.cg);
     int4 *s_info = reinterpret_cast<int4 *>(smem + Lo.info);
     int *s_sd = reinterpret_cast<int *>(smem + Lo.sd);
     T *s_buf = reinterpret_cast<T *>(smem + Lo.buf);
-    const long long stride_state = A.sstate;
-    const long long stride_buf = stride_state * S;
+    const int stride_state = (int)A.sstate;  // shared-memory offsets fit in 32 bits
+    const int stride_buf = stride_state * S;
+    const int TF = (int)A.TF;
     constexpr int S2 = S * S;
 
     const int tid = threadIdx.x, nth = blockDim.x;
@@ -133,7 +136,7 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
         for (int s = 0; s < S; ++s) {
             T *base = s_buf + b * stride_buf + s * stride_state;
             for (int i = tid; i < A.pad; i += nth) base[i] = (T)0;
-            for (long long i = A.pad + A.TF + tid; i < stride_state; i += nth) base[i] = (T)0;
+            for (int i = A.pad + TF + tid; i < stride_state; i += nth) base[i] = (T)0;
         }
     __syncthreads();
     // per-CTA step tables
@@ -169,6 +172,19 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
             fr[q] = st->fast_row[q];
         }
         s_info[i] = make_int4(st->stride, (int)w, fr[0] | (fr[1] << 16), fr[2] | (fr[3] << 16));
+    }
+    __syncthreads();
+    // direct groups: the sum of their steps' blocks (uniform over the tile)
+    for (int q = A.nstaged + tid; q < A.ngroups; q += nth) {
+        const SlabGroup *G = A.groups + q;
+        T C[S2];
+#pragma unroll
+        for (int ab = 0; ab < S2; ++ab) C[ab] = 0;
+        for (int i = G->step_begin; i < G->step_end; ++i)
+#pragma unroll
+            for (int ab = 0; ab < S2; ++ab) C[ab] += s_cm[i * S2 + ab];
+#pragma unroll
+        for (int ab = 0; ab < S2; ++ab) s_cg[(q - A.nstaged) * S2 + ab] = C[ab];
     }
 
     auto group_valid = [&](int g) {
@@ -214,15 +230,14 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
         }
         pk[k] = p;
     }
+    // digits of the fast fields other than the slowest one, identical for every k in the
+    // column mapping
+    const uint32_t pkt = pk[0] & ~0xFFu;
     T acc[S][SLAB_RPT];
-    T xown[S][SLAB_RPT];
 #pragma unroll
     for (int a = 0; a < S; ++a)
 #pragma unroll
-        for (int k = 0; k < SLAB_RPT; ++k) {
-            acc[a][k] = 0;
-            xown[a][k] = 0;
-        }
+        for (int k = 0; k < SLAB_RPT; ++k) acc[a][k] = 0;
 
     unsigned phase_bits = 0;  // bit b = parity of the next completion of buffer b
     int g = 0, bi = 0;
@@ -244,11 +259,7 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
             const SlabGroup *G = A.groups + q;
             T C[S2];
 #pragma unroll
-            for (int ab = 0; ab < S2; ++ab) C[ab] = 0;
-            const int sb = G->step_begin, se = G->step_end;
-            for (int i = sb; i < se; ++i)
-#pragma unroll
-                for (int ab = 0; ab < S2; ++ab) C[ab] += s_cm[i * S2 + ab];
+            for (int ab = 0; ab < S2; ++ab) C[ab] = s_cg[(q - A.nstaged) * S2 + ab];
             const long long base = (tile + G->tile_shift) * A.TF;
             const unsigned smask = G->state_mask;
 #pragma unroll
@@ -257,8 +268,7 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
                 T xb[SLAB_RPT];
                 const T *src = x + b * A.dimen + base + tid;
 #pragma unroll
-                for (int k = 0; k < SLAB_RPT; ++k)
-                    xb[k] = ((long long)k * nth + tid < A.TF) ? __ldcg(src + (long long)k * nth) : (T)0;
+                for (int k = 0; k < SLAB_RPT; ++k) xb[k] = (k * nth + tid < TF) ? __ldcg(src + k * nth) : (T)0;
 #pragma unroll
                 for (int a = 0; a < S; ++a)
                     if (C[a * S + b] != (T)0) {
@@ -280,13 +290,11 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
         const T *buf = s_buf + bi * stride_buf + A.pad;
         if (g == 0) {
             // diagonal section: harmonic energy, constants and zero-shift even terms
+            T xown[S][SLAB_RPT];
 #pragma unroll
             for (int a = 0; a < S; ++a)
 #pragma unroll
-                for (int k = 0; k < SLAB_RPT; ++k) {
-                    const long long r = (long long)k * nth + tid;
-                    xown[a][k] = r < A.TF ? buf[a * stride_state + r] : (T)0;
-                }
+                for (int k = 0; k < SLAB_RPT; ++k) xown[a][k] = buf[a * stride_state + k * nth + tid];
             T ekin[SLAB_RPT];
             {
                 T slow_ekin = 0;
@@ -343,7 +351,26 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
             T e[SLAB_RPT];
 #pragma unroll
             for (int k = 0; k < SLAB_RPT; ++k) e[k] = 1;
-            if (nfa >= 1) {
+            if (nfa >= 1 && A.cols) {
+                // the slowest fast mode's digit is k (uniform table reads), the others are fixed
+                T et = 1;
+                int mrow = -1;
+                for (int q = 0; q < nfa; ++q) {
+                    const int f = info_field(w, q);
+                    const int off = q == 0 ? (inf.z & 0xFFFF)
+                                           : q == 1 ? (int)((unsigned)inf.z >> 16)
+                                                    : q == 2 ? (inf.w & 0xFFFF) : (int)((unsigned)inf.w >> 16);
+                    if (f == 0) mrow = off;
+                    else et *= s_ftab[off + (int)((pkt >> (8 * f)) & 0xFFu)];
+                }
+                if (mrow >= 0) {
+#pragma unroll
+                    for (int k = 0; k < SLAB_RPT; ++k) e[k] = et * s_ftab[mrow + k];
+                } else {
+#pragma unroll
+                    for (int k = 0; k < SLAB_RPT; ++k) e[k] = et;
+                }
+            } else if (nfa >= 1) {
                 const T *row = s_ftab + (inf.z & 0xFFFF);
                 const int sh = 8 * info_field(w, 0);
 #pragma unroll
@@ -367,9 +394,9 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
             for (int b = 0; b < S; ++b) {
                 if (!((cols >> b) & 1u)) continue;
                 T xb[SLAB_RPT];
-                const T *src = buf + b * stride_state + inf.x + tid;
+                const T *src = buf + (b * stride_state + inf.x + tid);
 #pragma unroll
-                for (int k = 0; k < SLAB_RPT; ++k) xb[k] = src[(long long)k * nth];
+                for (int k = 0; k < SLAB_RPT; ++k) xb[k] = src[k * nth];
                 if (nfa >= 1) {
 #pragma unroll
                     for (int k = 0; k < SLAB_RPT; ++k) xb[k] *= e[k];
@@ -404,8 +431,9 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
             const long long r = (long long)k * nth + tid;
             if (r < A.TF) {
                 const T v = acc[a][k] * sc;
-                y[a * A.dimen + tile * A.TF + r] = v;
-                part += ((double)xown[a][k] * (double)sc) * (double)v;
+                const long long gi = a * A.dimen + tile * A.TF + r;
+                y[gi] = v;
+                if (alpha_part) part += ((double)__ldcg(x + gi) * (double)sc) * (double)v;
             }
         }
     if (alpha_part) {
@@ -441,6 +469,7 @@ static SlabArgs<T> slab_args(const SlabPlan &sp, const Plan &pl) {
     a.slow_nfunc = sp.d_slow_nfunc;
     a.fast_shft = sp.d_fast_shft;
     a.m = sp.m;
+    a.cols = sp.cols;
     a.nF = sp.nF;
     a.pad = sp.pad;
     a.TF = sp.TF;

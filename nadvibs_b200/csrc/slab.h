@@ -58,6 +58,9 @@ struct SlabPlan {
     long long TF = 0;          // rows per tile
     long long ntiles = 0;
     int threads = 0;
+    int cols = 0;              // 1: threads = shft(m), row r = k*threads + tid, so the digit of the
+                               // slowest fast mode is k and the other fast digits depend on tid only
+    int frow_len = 0;          // entries per fast-table row (>= SLAB_RPT)
     int pad = 0;               // zero halo (elements) before/after each staged state tile
     long long sstate = 0;      // elements per state in a buffer: pad + TF + pad + tail
     int nfrows = 0;            // fast table rows
@@ -92,10 +95,10 @@ struct SlabPlan {
 
 // Dynamic shared-memory layout of the slab kernel (byte offsets), shared by host and device.
 struct SlabLayout {
-    size_t ftab, etab, cm, info, sd, buf, total;
+    size_t ftab, etab, cm, cg, info, sd, buf, total;
 };
-__host__ __device__ inline SlabLayout slab_layout(long long ftab_len, long long etab_len, long long nsteps, int S,
-                                                  int m, long long sstate, int eb) {
+__host__ __device__ inline SlabLayout slab_layout(long long ftab_len, long long etab_len, long long nsteps,
+                                                  long long ndirect, int S, int m, long long sstate, int eb) {
     SlabLayout L;
     size_t off = 64;  // mbarriers
     L.ftab = off;
@@ -104,6 +107,8 @@ __host__ __device__ inline SlabLayout slab_layout(long long ftab_len, long long 
     off += (size_t)etab_len * eb;
     L.cm = off;
     off += (size_t)nsteps * S * S * eb;
+    L.cg = off;
+    off += (size_t)ndirect * S * S * eb;
     off = (off + 15) / 16 * 16;
     L.info = off;
     off += (size_t)nsteps * 16;

@@ -22,8 +22,8 @@ static int slab_threads(long long TF) {
 }
 
 size_t slab_smem(const SlabPlan &sp, const Plan &pl, int eb) {
-    return slab_layout((long long)sp.ftab.size(), (long long)pl.h_etab.size(), (long long)sp.steps.size(), pl.S, sp.m,
-                       sp.sstate, eb)
+    return slab_layout((long long)sp.ftab.size(), (long long)pl.h_etab.size(), (long long)sp.steps.size(),
+                       (long long)(sp.groups.size() - sp.nstaged), pl.S, sp.m, sp.sstate, eb)
         .total;
 }
 
@@ -58,6 +58,14 @@ bool slab_build(SlabPlan &sp, const Plan &pl, const System &sys, int quirk_cubic
     if (sp.TF < 64) return false;                             // too little work per CTA
     if (sp.TF % 4 != 0 || sys.dimen % 4 != 0) return false;  // 16-byte TMA alignment
     sp.threads = slab_threads(sp.TF);
+    {
+        const long long sm = sys.shft[m];  // rows per value of the slowest fast mode
+        if (sm % 32 == 0 && sm <= slab_max_threads(eb) && sys.nfunc[m] <= SLAB_RPT) {
+            sp.threads = (int)sm;
+            sp.cols = 1;
+        }
+    }
+    sp.frow_len = std::max(pl.nmax, SLAB_RPT);
     for (int l = 0; l < m; ++l) {
         sp.slow_tshft.push_back(sys.shft[l] / sp.TF);
         sp.slow_nfunc.push_back((int)sys.nfunc[l]);
@@ -74,10 +82,10 @@ bool slab_build(SlabPlan &sp, const Plan &pl, const System &sys, int quirk_cubic
         auto key = std::make_tuple(j, p, s);
         auto it = frow.find(key);
         if (it != frow.end()) return it->second;
-        const int r = (int)frow.size() * pl.nmax;  // element offset of the row
+        const int r = (int)frow.size() * sp.frow_len;  // element offset of the row
         frow[key] = r;
         const int nf = sp.fast_nfunc[j];
-        for (int n = 0; n < pl.nmax; ++n) {
+        for (int n = 0; n < sp.frow_len; ++n) {
             double v = 0.0;
             if (n < nf && n + s >= 0 && n + s < nf) {
                 const int lo = std::min(n, n + s);
@@ -203,7 +211,7 @@ bool slab_build(SlabPlan &sp, const Plan &pl, const System &sys, int quirk_cubic
         sp.groups.push_back(G);
     }
     sp.nfrows = (int)frow.size();
-    if (sp.ftab.empty()) sp.ftab.assign(pl.nmax, 0.0);
+    if (sp.ftab.empty()) sp.ftab.assign(sp.frow_len, 0.0);
     if (sp.ftab.size() > 65535) return false;  // fast row offsets are packed in 16 bits
     sp.smem_bytes[0] = slab_smem(sp, pl, 8);
     sp.smem_bytes[1] = slab_smem(sp, pl, 4);
