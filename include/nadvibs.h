@@ -68,7 +68,10 @@ typedef struct nvb_options {
                               does (Source/top.f90:752-754); 0: symmetric */
     int64_t archive_max;   /* max Lanczos vectors kept on the device for Ritz vectors /
                               re-orthogonalisation; 0 = none (two-pass Ritz vectors) */
-    int64_t hv_kernel;     /* 0 = automatic choice; 1 = gather kernel; 2 = tiled kernel */
+    int64_t hv_kernel;     /* 0 = automatic choice (factorised quadratic kernel where the
+                              system suits it, else the slab-tiled kernel, else gather);
+                              1 = gather kernel; 2 = slab-tiled kernel; 3 = factorised
+                              quadratic kernel (ordr <= 2, state-diagonal bilinear terms) */
     int64_t seed;          /* seed of the omega-recurrence noise (the reference is unseeded) */
 } nvb_options;
 

@@ -115,7 +115,12 @@ static void create_common(nvb_handle *h, const nvb_params &p, const double *omeg
     h->precision = (int)h->opt.precision;
     plan_build(h->plan, h->sys, (int)h->opt.quirk_cubic, (int)h->opt.quirk_lower);
     plan_upload(h->plan);
-    if (h->opt.hv_kernel != 1) {
+    if (h->opt.hv_kernel == 0 || h->opt.hv_kernel == 3) {
+        if (nvb::quad_build(h->quad, h->plan, h->sys)) nvb::quad_upload(h->quad);
+        if (h->opt.hv_kernel == 3 && !h->quad.ok)
+            fail(NVB_ERR_ARG, "factorised quadratic kernel requested but the system does not suit it");
+    }
+    if (h->opt.hv_kernel == 0 || h->opt.hv_kernel == 2) {
         for (int i = 0; i < 2; ++i)
             if (slab_build(h->slab[i], h->plan, h->sys, (int)h->opt.quirk_cubic, i == 0 ? 8 : 4)) slab_upload(h->slab[i]);
         if (h->opt.hv_kernel == 2 && !h->slab[0].ok && !h->slab[1].ok)
@@ -176,6 +181,7 @@ int nvb_destroy(nvb_handle *h) {
             plan_free(h->plan);
             slab_free(h->slab[0]);
             slab_free(h->slab[1]);
+            quad_free(h->quad);
             if (h->own_stream) cudaStreamDestroy(h->own_stream);
         }
     });

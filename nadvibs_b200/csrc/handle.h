@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "plan.h"
+#include "quad.h"
 #include "slab.h"
 
 struct nvb_handle {
@@ -13,6 +14,7 @@ struct nvb_handle {
     nvb_options opt{};
     nvb::Plan plan;
     nvb::SlabPlan slab[2];  // slab-tiled H.v plans for FP64 (0) and FP32 (1) vectors
+    nvb::QuadPlan quad;     // factorised quadratic H.v plan (both precisions)
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;

@@ -1,0 +1,561 @@
+// Factorised quadratic H.v kernel (see quad.h for the algebra).
+//
+// Warp-specialised persistent CTAs walk the tiles (fixed slow digits) with a stride of the
+// grid.  The last warp is the producer: one lane walks the same item sequence as the
+// consumers (per tile, per target state a: the own tile x_a, the other states' own tiles,
+// the slow +-1 / +-2 / bilinear neighbour tiles) and copies each valid item into the next
+// slot of a ring of shared-memory buffers with a TMA bulk copy completing on the slot's
+// "full" mbarrier, after the consumers released the slot on its "empty" mbarrier.  The other
+// warps are the consumers; a thread owns the pencil of mode m (rows r*shft(m) + tid) and
+// folds each item into registers:
+//   own x_a:      diagonal section, Z_l += G^aa_l x_a + Q^a_kl X_k x_a (fast k < l), squares;
+//   own x_b:      off-diagonal diagonal-section entries, Z_l += G^ab_l x_b, squares of x_b;
+//   slow +-1:     y_a += G^ab_k e x_b(p+-e_k), Z_l += Q^a_kl e x_a(p+-e_k);
+//   slow +-2:     y_a += R^ab_k e x_b(p+-2e_k);
+//   slow pairs:   y_a += Q^a_kl e x_a(p+-e_k+-e_l);
+// with e the tile's slow element factor.  Finally Z_l (l > m) goes to shared memory and
+// y_a += X_l Z_l (register shifts along m).  Out-of-basis neighbours have element factor 0
+// (the item is skipped by producer and consumers alike) and zero-filled halos.
+// Every wait is bounded: a wait that runs out raises a CTA abort flag, after which no thread
+// waits again and the kernel reports the failure through its error word.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "quad.h"
+
+namespace nvb {
+
+namespace {
+
+template <typename T>
+struct QuadArgs {
+    const T *blk;  // tab | G | R | Q | cst | omega
+    const int *slow;
+    const QuadItem *items;
+    const int *item_beg;
+    int *err;
+    int M, m, nmax, nv, pad, sstate, TF, ntiles, nslot, nitems;
+    long long dimen;
+    unsigned dpm;
+    QuadFast<T> F;
+};
+
+// consumers (<= 288 = 9 warps) + the producer warp: 10 warps keep <= 3 warps per SM sub-partition,
+// so a thread may hold up to 168 registers
+constexpr int QUAD_MAXTH = 288 + 32;
+constexpr int R = QUAD_RPT;
+constexpr int WAIT_LIMIT = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on a phase; gives up (and raises the abort flag) after WAIT_LIMIT polls, or
+// early once another thread raised it.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, volatile int *abort_flag) {
+    for (int i = 0; i < WAIT_LIMIT; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if ((i & 255) == 255 && *abort_flag) return false;
+    }
+    *abort_flag = 1;
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// barrier 1 among the consumer warps only (the producer never joins it)
+__device__ __forceinline__ void consumer_sync(int n) { asm volatile("bar.sync 1, %0;" ::"r"(n) : "memory"); }
+
+// element-table row of an item's (first or second) slow factor
+__device__ __forceinline__ int item_row(int kind, int s) {
+    return kind == QI_SLOW2 ? (s > 0 ? 2 : 3) : (s > 0 ? 0 : 1);
+}
+
+template <typename T, int S, int NF>
+__global__ void __launch_bounds__(QUAD_MAXTH, 1)
+    k_hv_quad(const QuadArgs<T> A, const T *__restrict__ x, T *__restrict__ y, const double *__restrict__ scale_dev,
+              double *__restrict__ alpha_part) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int M = A.M, m = A.m, nmax = A.nmax, sst = A.sstate, TF = A.TF, NS = A.nslot, pad = A.pad;
+    const QuadLayout Lo = quad_layout(M, S, nmax, m, NF, sst, (int)sizeof(T), NS, A.nitems);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = full + QUAD_MAXSLOT;
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + 2 * QUAD_MAXSLOT * 8);
+    T *s_tab = reinterpret_cast<T *>(smem + Lo.tab);
+    T *s_G = reinterpret_cast<T *>(smem + Lo.G);
+    T *s_R = reinterpret_cast<T *>(smem + Lo.R);
+    T *s_Q = reinterpret_cast<T *>(smem + Lo.Q);
+    T *s_cst = reinterpret_cast<T *>(smem + Lo.cst);
+    T *s_om = reinterpret_cast<T *>(smem + Lo.om);
+    int *s_sl = reinterpret_cast<int *>(smem + Lo.sd);  // slow tile strides [MAXSL], nfunc [MAXSL]
+    T *s_se = reinterpret_cast<T *>(smem + Lo.se);      // [2][MAXSL][5] slow element factors of a tile
+    T *s_dt = reinterpret_cast<T *>(smem + Lo.dt);      // [2][S*S+1] slow diagonal block, energy
+    QuadItem *s_it = reinterpret_cast<QuadItem *>(smem + Lo.items);
+    int *s_ib = reinterpret_cast<int *>(smem + Lo.items + A.nitems * (int)sizeof(QuadItem));
+    T *s_ring = reinterpret_cast<T *>(smem + Lo.ring);  // [NS][sst]
+    T *s_z = reinterpret_cast<T *>(smem + Lo.z);        // [NF-1][sst] Z_l, l > m
+    const int tid = threadIdx.x;
+    const int nc = (int)blockDim.x - 32;  // consumer threads = shft(m)
+    const long long N = A.dimen;
+    const QuadFast<T> &F = A.F;
+    constexpr int SS = S * S;
+    const int *tsh = s_sl, *snf = s_sl + QUAD_MAXSL;
+
+    {
+        const int ntab = M * 5 * nmax, nG = M * SS, nQ = M * M * S;
+        const T *src = A.blk;
+        for (int i = tid; i < ntab; i += blockDim.x) s_tab[i] = src[i];
+        src += ntab;
+        for (int i = tid; i < nG; i += blockDim.x) s_G[i] = src[i];
+        src += nG;
+        for (int i = tid; i < nG; i += blockDim.x) s_R[i] = src[i];
+        src += nG;
+        for (int i = tid; i < nQ; i += blockDim.x) s_Q[i] = src[i];
+        src += nQ;
+        for (int i = tid; i < SS; i += blockDim.x) s_cst[i] = src[i];
+        src += SS;
+        for (int i = tid; i < M; i += blockDim.x) s_om[i] = src[i];
+        for (int i = tid; i < m; i += blockDim.x) {
+            s_sl[i] = A.slow[i];
+            s_sl[QUAD_MAXSL + i] = A.slow[m + i];
+        }
+        for (int i = tid; i < A.nitems; i += blockDim.x) s_it[i] = A.items[i];
+        for (int i = tid; i <= S; i += blockDim.x) s_ib[i] = A.item_beg[i];
+        const int nz = (NS + (NF > 1 ? NF - 1 : 1)) * sst;  // ring and Z are contiguous
+        for (int i = tid; i < nz; i += blockDim.x) s_ring[i] = (T)0;
+    }
+    if (tid == 0) {
+        for (int i = 0; i < NS; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], (unsigned)(nc >> 5));
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    fence_proxy_async();
+    __syncthreads();
+
+    if (tid >= nc) {
+        // ---------------- producer ----------------
+        if (tid == nc) {
+            const unsigned bytes = (unsigned)TF * (unsigned)sizeof(T);
+            const int nit = s_ib[S];
+            int slot = 0;
+            unsigned ph = 0;
+            long long issued = 0;
+            bool stop = false;
+            for (int tile = blockIdx.x; tile < A.ntiles && !stop; tile += gridDim.x)
+                for (int it = 0; it < nit; ++it) {
+                    const QuadItem q = s_it[it];
+                    if (q.kind != QI_OWN) {
+                        const int dk = (tile / tsh[q.k]) % snf[q.k];
+                        bool ok = s_tab[(q.k * 5 + item_row(q.kind, q.sk)) * nmax + dk] != (T)0;
+                        if (q.kind == QI_PAIR) {
+                            const int dl = (tile / tsh[q.l]) % snf[q.l];
+                            ok = ok && s_tab[(q.l * 5 + item_row(q.kind, q.sl)) * nmax + dl] != (T)0;
+                        }
+                        if (!ok) continue;
+                    }
+                    if (!mbar_wait(&empty[slot], ph ^ 1u, abort_flag)) {
+                        stop = true;
+                        break;
+                    }
+                    fence_proxy_async();
+                    mbar_expect_tx(&full[slot], bytes);
+                    bulk_g2s(s_ring + slot * sst + pad, x + q.b * N + (long long)(tile + q.tshift) * TF, bytes,
+                             &full[slot]);
+                    ++issued;
+                    if (++slot == NS) {
+                        slot = 0;
+                        ph ^= 1u;
+                    }
+                }
+            if (stop) {
+                // the copies still in flight complete on their full barriers: wait for them
+                // (bounded) before the CTA leaves
+                const long long n = issued < NS ? issued : NS;
+                for (long long i = issued - n; i < issued; ++i) {
+                    const int s = (int)(i % NS);
+                    const unsigned p = (unsigned)((i / NS) & 1);
+                    for (int w = 0; w < WAIT_LIMIT && !mbar_try(&full[s], p); ++w) {
+                    }
+                }
+                atomicExch(A.err, 1);
+            }
+        }
+        return;
+    }
+
+    // ---------------- consumers ----------------
+    int dj[NF];
+    T e1p[NF], e1m[NF];
+#pragma unroll
+    for (int j = 0; j < NF; ++j) {
+        dj[j] = 0;
+        e1p[j] = e1m[j] = (T)0;
+        if (j >= 1) {
+            dj[j] = (tid / F.sh[j]) % F.nf[j];
+            e1p[j] = s_tab[((m + j) * 5 + 0) * nmax + dj[j]];
+            e1m[j] = s_tab[((m + j) * 5 + 1) * nmax + dj[j]];
+        }
+    }
+    const T sc = scale_dev ? (T)(*scale_dev) : (T)1;
+    const int nv = A.nv;
+    double part = 0.0;
+    int slot = 0;
+    unsigned ph = 0;
+    int tp = 0;
+    for (int tile = blockIdx.x; tile < A.ntiles; tile += gridDim.x, tp ^= 1) {
+        // the tile's slow element factors and the slow part of the diagonal block
+        if (tid < m) {
+            const int l = tid;
+            const int d = (tile / tsh[l]) % snf[l];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) s_se[(tp * QUAD_MAXSL + l) * 5 + q] = s_tab[(l * 5 + q) * nmax + d];
+        } else if (tid >= 32 && tid < 32 + SS + 1) {
+            const int ab = tid - 32;
+            T v = 0;
+            if (ab < SS) {
+                v = s_cst[ab];
+                if ((A.dpm >> ab) & 1u)
+                    for (int l = 0; l < m; ++l) {
+                        const int d = (tile / tsh[l]) % snf[l];
+                        v += s_R[l * SS + ab] * s_tab[(l * 5 + 4) * nmax + d];
+                    }
+            } else {
+                for (int l = 0; l < m; ++l) {
+                    const int d = (tile / tsh[l]) % snf[l];
+                    v += s_om[l] * ((T)d + (T)0.5);
+                }
+            }
+            s_dt[tp * (SS + 1) + ab] = v;
+        }
+        consumer_sync(nc);
+        const T *se = s_se + tp * QUAD_MAXSL * 5;
+        const T *dt = s_dt + tp * (SS + 1);
+        const long long tbase = (long long)tile * TF;
+#pragma unroll
+        for (int a = 0; a < S; ++a) {
+            T xr[R], acc[R], Z[NF][R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                xr[r] = acc[r] = (T)0;
+#pragma unroll
+                for (int j = 0; j < NF; ++j) Z[j][r] = (T)0;
+            }
+            T hj[NF];  // <n|x^2|n> of the thread's fast digits (j >= 1)
+#pragma unroll
+            for (int j = 0; j < NF; ++j) hj[j] = (T)dj[j] + (T)0.5;
+            const int iend = s_ib[a + 1];
+            for (int it = s_ib[a]; it < iend; ++it) {
+                const QuadItem q = s_it[it];
+                T e = (T)1;
+                if (q.kind != QI_OWN) {
+                    e = se[q.k * 5 + item_row(q.kind, q.sk)];
+                    if (q.kind == QI_PAIR) e *= se[q.l * 5 + item_row(q.kind, q.sl)];
+                    if (e == (T)0) continue;
+                }
+                const bool ok = mbar_wait(&full[slot], ph, abort_flag);
+                const T *buf = s_ring + slot * sst + pad;
+                if (ok) {
+                    const int b = q.b;
+                    if (q.kind == QI_OWN && b == a) {
+#pragma unroll
+                        for (int r = 0; r < R; ++r) xr[r] = buf[r * nc + tid];
+                        // diagonal section
+                        T ek = dt[SS], daa = dt[a * S + a];
+#pragma unroll
+                        for (int j = 1; j < NF; ++j) {
+                            ek += F.om[j] * hj[j];
+                            daa += F.R[j][a][a] * hj[j];
+                        }
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            const T h = (T)r + (T)0.5;
+                            acc[r] += (daa + F.R[0][a][a] * h + ek + F.om[0] * h) * xr[r];
+                        }
+                        // fast linear, own state
+#pragma unroll
+                        for (int j = 0; j < NF; ++j) {
+                            const T g = F.G[j][a][a];
+                            if (g != (T)0) {
+#pragma unroll
+                                for (int r = 0; r < R; ++r) Z[j][r] += g * xr[r];
+                            }
+                        }
+                        // fast bilinear: Z_l += Q^a_il X_i x_a (fast i < l)
+#pragma unroll
+                        for (int i = 0; i + 1 < NF; ++i) {
+                            bool any = false;
+#pragma unroll
+                            for (int j = i + 1; j < NF; ++j) any |= F.Q[i][j][a] != (T)0;
+                            if (!any) continue;
+                            T V[R];
+#pragma unroll
+                            for (int r = 0; r < R; ++r) {
+                                if (i == 0) {
+                                    T v = (T)0;
+                                    if (r + 1 < R) v += F.em[0][r] * xr[r + 1];
+                                    if (r >= 1) v += F.em[1][r] * xr[r - 1];
+                                    V[r] = v;
+                                } else {
+                                    const T *p = buf + r * nc + tid;
+                                    V[r] = e1p[i] * p[F.sh[i]] + e1m[i] * p[-F.sh[i]];
+                                }
+                            }
+#pragma unroll
+                            for (int j = i + 1; j < NF; ++j) {
+                                const T qq = F.Q[i][j][a];
+                                if (qq == (T)0) continue;
+#pragma unroll
+                                for (int r = 0; r < R; ++r) Z[j][r] += qq * V[r];
+                            }
+                        }
+                        // fast squares, own state
+#pragma unroll
+                        for (int j = 0; j < NF; ++j) {
+                            const T rr = F.R[j][a][a];
+                            if (rr == (T)0) continue;
+                            T e2p = (T)0, e2m = (T)0;
+                            if (j >= 1) {
+                                e2p = s_tab[((m + j) * 5 + 2) * nmax + dj[j]];
+                                e2m = s_tab[((m + j) * 5 + 3) * nmax + dj[j]];
+                            }
+#pragma unroll
+                            for (int r = 0; r < R; ++r) {
+                                T v = (T)0;
+                                if (j == 0) {
+                                    if (r + 2 < R) v += F.em[2][r] * xr[r + 2];
+                                    if (r >= 2) v += F.em[3][r] * xr[r - 2];
+                                } else {
+                                    const T *p = buf + r * nc + tid;
+                                    v = e2p * p[2 * F.sh[j]] + e2m * p[-2 * F.sh[j]];
+                                }
+                                acc[r] += rr * v;
+                            }
+                        }
+                    } else if (q.kind == QI_OWN) {
+                        // another state's own tile
+                        T xb[R];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) xb[r] = buf[r * nc + tid];
+                        if ((A.dpm >> (a * S + b)) & 1u) {
+                            T dab = dt[a * S + b];
+#pragma unroll
+                            for (int j = 1; j < NF; ++j) dab += F.R[j][a][b] * hj[j];
+                            const T r0 = F.R[0][a][b];
+#pragma unroll
+                            for (int r = 0; r < R; ++r) acc[r] += (dab + r0 * ((T)r + (T)0.5)) * xb[r];
+                        }
+#pragma unroll
+                        for (int j = 0; j < NF; ++j) {
+                            const T g = F.G[j][a][b];
+                            if (g != (T)0) {
+#pragma unroll
+                                for (int r = 0; r < R; ++r) Z[j][r] += g * xb[r];
+                            }
+                            const T rr = F.R[j][a][b];
+                            if (rr != (T)0) {
+                                T e2p = (T)0, e2m = (T)0;
+                                if (j >= 1) {
+                                    e2p = s_tab[((m + j) * 5 + 2) * nmax + dj[j]];
+                                    e2m = s_tab[((m + j) * 5 + 3) * nmax + dj[j]];
+                                }
+#pragma unroll
+                                for (int r = 0; r < R; ++r) {
+                                    T v = (T)0;
+                                    const T *p = buf + r * nc + tid;
+                                    if (j == 0) {
+                                        if (r + 2 < R) v += F.em[2][r] * p[2 * nc];
+                                        if (r >= 2) v += F.em[3][r] * p[-2 * nc];
+                                    } else {
+                                        v = e2p * p[2 * F.sh[j]] + e2m * p[-2 * F.sh[j]];
+                                    }
+                                    acc[r] += rr * v;
+                                }
+                            }
+                        }
+                    } else {
+                        T v[R];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) v[r] = buf[r * nc + tid];
+                        T c;
+                        if (q.kind == QI_SLOW1) c = s_G[q.k * SS + a * S + b];
+                        else if (q.kind == QI_SLOW2) c = s_R[q.k * SS + a * S + b];
+                        else c = s_Q[(q.k * M + q.l) * S + a];
+                        c *= e;
+                        if (c != (T)0) {
+#pragma unroll
+                            for (int r = 0; r < R; ++r) acc[r] += c * v[r];
+                        }
+                        if (q.kind == QI_SLOW1 && b == a) {
+#pragma unroll
+                            for (int j = 0; j < NF; ++j) {
+                                const T qz = s_Q[(q.k * M + m + j) * S + a] * e;
+                                if (qz != (T)0) {
+#pragma unroll
+                                    for (int r = 0; r < R; ++r) Z[j][r] += qz * v[r];
+                                }
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+                if ((tid & 31) == 0) mbar_arrive(&empty[slot]);
+                if (++slot == NS) {
+                    slot = 0;
+                    ph ^= 1u;
+                }
+            }
+            // y_a += X_l Z_l
+#pragma unroll
+            for (int j = 1; j < NF; ++j)
+#pragma unroll
+                for (int r = 0; r < R; ++r) s_z[(j - 1) * sst + pad + r * nc + tid] = r < nv ? Z[j][r] : (T)0;
+            consumer_sync(nc);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                T v = acc[r];
+                if (r + 1 < R) v += F.em[0][r] * Z[0][r + 1];
+                if (r >= 1) v += F.em[1][r] * Z[0][r - 1];
+#pragma unroll
+                for (int j = 1; j < NF; ++j) {
+                    const T *p = s_z + (j - 1) * sst + pad + r * nc + tid;
+                    v += e1p[j] * p[F.sh[j]] + e1m[j] * p[-F.sh[j]];
+                }
+                acc[r] = v;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (r < nv) {
+                    const T v = acc[r] * sc;
+                    y[a * N + tbase + r * nc + tid] = v;
+                    if (alpha_part) part += ((double)xr[r] * (double)sc) * (double)v;
+                }
+            consumer_sync(nc);  // s_z is rewritten by the next state
+        }
+    }
+    if (*abort_flag && tid == 0) atomicExch(A.err, 1);
+    if (alpha_part) {
+        __shared__ double red[32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if ((tid & 31) == 0) red[tid >> 5] = part;
+        consumer_sync(nc);
+        if (tid < 32) {
+            double v = tid < (nc >> 5) ? red[tid] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (tid == 0) alpha_part[blockIdx.x] = v;
+        }
+    }
+}
+
+template <typename T>
+QuadArgs<T> quad_args(const QuadPlan &qp) {
+    QuadArgs<T> a{};
+    a.slow = qp.d_slow;
+    a.items = qp.d_items;
+    a.item_beg = qp.d_item_beg;
+    a.err = qp.d_err;
+    a.M = qp.M;
+    a.m = qp.m;
+    a.nmax = qp.nmax;
+    a.nv = qp.nv;
+    a.pad = qp.pad;
+    a.sstate = qp.sstate;
+    a.TF = qp.TF;
+    a.ntiles = qp.ntiles;
+    a.nitems = (int)qp.items.size();
+    a.dimen = qp.dimen;
+    a.dpm = qp.dpm;
+    if constexpr (sizeof(T) == 8) {
+        a.blk = (const T *)qp.d_blk;
+        a.F = qp.fast_d;
+        a.nslot = qp.nslot[0];
+    } else {
+        a.blk = (const T *)qp.d_blk_f;
+        a.F = qp.fast_f;
+        a.nslot = qp.nslot[1];
+    }
+    return a;
+}
+
+template <typename T, int S, int NF>
+int launch_q(QuadPlan &qp, const T *x, T *y, const double *sc, double *ap, cudaStream_t st) {
+    const int idx = sizeof(T) == 8 ? 0 : 1;
+    const size_t smem = qp.smem[idx];
+    const int threads = qp.threads + 32;
+    auto kern = k_hv_quad<T, S, NF>;
+    if (qp.grid[idx] == 0) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int dev = 0, nsm = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem);
+        if (per < 1) fail(NVB_ERR_CUDA, "quadratic H.v kernel does not fit on a multiprocessor");
+        long long g = (long long)nsm * per;
+        if (g > qp.ntiles) g = qp.ntiles;
+        qp.grid[idx] = (int)g;
+    }
+    kern<<<qp.grid[idx], threads, smem, st>>>(quad_args<T>(qp), x, y, sc, ap);
+    return qp.grid[idx];
+}
+
+template <typename T, int S>
+int launch_qs(QuadPlan &qp, const T *x, T *y, const double *sc, double *ap, cudaStream_t st) {
+    switch (qp.nF) {
+    case 2: return launch_q<T, S, 2>(qp, x, y, sc, ap, st);
+    case 3: return launch_q<T, S, 3>(qp, x, y, sc, ap, st);
+    case 4: return launch_q<T, S, 4>(qp, x, y, sc, ap, st);
+    default: fail(NVB_ERR_ARG, "quadratic kernel: unsupported number of fast modes");
+    }
+}
+
+}  // namespace
+
+template <typename T>
+int quad_launch(QuadPlan &qp, const T *x, T *y, const double *scale, double *alpha_part, cudaStream_t st) {
+    switch (qp.S) {
+    case 1: return launch_qs<T, 1>(qp, x, y, scale, alpha_part, st);
+    case 2: return launch_qs<T, 2>(qp, x, y, scale, alpha_part, st);
+    case 3: return launch_qs<T, 3>(qp, x, y, scale, alpha_part, st);
+    case 4: return launch_qs<T, 4>(qp, x, y, scale, alpha_part, st);
+    default: fail(NVB_ERR_ARG, "quadratic kernel supports up to 4 states");
+    }
+}
+
+template int quad_launch<double>(QuadPlan &, const double *, double *, const double *, double *, cudaStream_t);
+template int quad_launch<float>(QuadPlan &, const float *, float *, const double *, double *, cudaStream_t);
+
+}  // namespace nvb

@@ -141,6 +141,16 @@ void hv_any(nvb_handle *h, const void *x, void *y, int dtype, const double *scal
     if (alpha_part == nullptr && nblocks_out) *nblocks_out = 0;
     const SlabPlan &sp = h->slab[dtype == NVB_DTYPE_F32 ? 1 : 0];
     const bool aligned = ((uintptr_t)x % 16) == 0;
+    if (h->quad.ok && aligned) {
+        int nb;
+        if (dtype == NVB_DTYPE_F64)
+            nb = quad_launch<double>(h->quad, (const double *)x, (double *)y, scale_dev, alpha_part, h->stream);
+        else
+            nb = quad_launch<float>(h->quad, (const float *)x, (float *)y, scale_dev, alpha_part, h->stream);
+        CK(cudaGetLastError());
+        if (nblocks_out) *nblocks_out = nb;
+        return;
+    }
     if (sp.ok && aligned && h->opt.hv_kernel != 1) {
         if (dtype == NVB_DTYPE_F64)
             slab_launch<double>(sp, h->plan, (const double *)x, (double *)y, scale_dev, alpha_part, h->stream);
@@ -158,8 +168,13 @@ void hv_any(nvb_handle *h, const void *x, void *y, int dtype, const double *scal
     if (nblocks_out) *nblocks_out = hv_gather_blocks(h->plan);
 }
 
-// A slab kernel whose tile copy never completed sets its error flag and stops early.
+// A tiled kernel whose tile copy never completed sets its error flag and stops early.
 void check_kernel_flags(nvb_handle *h) {
+    if (h->quad.ok && h->quad.d_err) {
+        int e = 0;
+        CK(cudaMemcpy(&e, h->quad.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) fail(NVB_ERR_CUDA, "quadratic H.v: a shared-memory tile copy did not complete (kernel gave up waiting)");
+    }
     for (int i = 0; i < 2; ++i)
         if (h->slab[i].ok && h->slab[i].d_err) {
             int e = 0;

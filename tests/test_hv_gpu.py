@@ -89,6 +89,45 @@ def test_hv_slab_kernel_matches_oracle(seed, nstates, basis, ordr, quirks):
     assert np.abs(y32 - y_ref).max() <= TOL32 * scale
 
 
+QUAD = [(61, 1, [4, 3, 5, 4, 8, 8]), (62, 2, [3, 3, 3, 2, 4, 8, 4]), (63, 3, [6, 5, 4, 8, 8]),
+        (64, 4, [5, 4, 4, 2, 8, 4]), (65, 3, [5, 4, 8, 8, 4, 2])]
+
+
+@pytest.mark.parametrize("seed,nstates,basis", QUAD)
+@pytest.mark.parametrize("quirks", [(1, 1), (0, 0)])
+def test_hv_quadratic_kernel_matches_oracle(seed, nstates, basis, quirks):
+    """Quadratic systems with state-diagonal bilinear terms (off-diagonal blocks: constants,
+    linear terms and squares) through the factorised kernel (hv_kernel=3 forces it; creation
+    fails if the system does not suit it), against the oracle and the gather kernel.  The
+    bases put 1-3 modes on the slow side, pencils of 2-8 rows and 2-level modes."""
+    cfg = synth.random_small(seed, nstates, basis, 2, offdiag_bilinear=False)
+    om, cc, pot = synth.draw_small(cfg)
+    S = O.system_from_arrays(basis, nstates, 2, om, cc, pot, quirk_cubic=bool(quirks[0]),
+                             quirk_lower=bool(quirks[1]))
+    x = np.random.default_rng(seed).normal(size=S.ntotal)
+    y_ref = S.hv(x, nthreads=8)
+    scale = np.abs(y_ref).max()
+    with _handle(_params(cfg), om, cc, pot, quirk_cubic=quirks[0], quirk_lower=quirks[1], hv_kernel=3) as h:
+        y64 = _hv_gpu(h, x)
+        y32 = _hv_gpu(h, x, torch.float32)
+    with _handle(_params(cfg), om, cc, pot, quirk_cubic=quirks[0], quirk_lower=quirks[1], hv_kernel=1) as hg:
+        g64 = _hv_gpu(hg, x)
+    assert np.abs(g64 - y_ref).max() <= TOL64 * scale
+    assert np.abs(y64 - y_ref).max() <= TOL64 * scale
+    assert np.abs(y32 - y_ref).max() <= TOL32 * scale
+
+
+def test_hv_quadratic_kernel_rejects_unsuited_systems():
+    """Bilinear inter-state couplings, cubic terms or a basis without a 32-aligned pencil
+    stride cannot use the factorised kernel: forcing it fails at creation."""
+    for basis, ordr, bil in [([4, 3, 5, 4, 8, 8], 2, True), ([4, 3, 5, 4, 8, 8], 3, False),
+                             ([8, 8, 6, 6], 2, False)]:
+        cfg = synth.random_small(66, 2, basis, ordr, offdiag_bilinear=bil, zero_frac=0.0)
+        om, cc, pot = synth.draw_small(cfg)
+        with pytest.raises(L.NvbError):
+            _handle(_params(cfg), om, cc, pot, hv_kernel=3).close()
+
+
 @pytest.mark.parametrize("n", [1, 4])
 def test_hv_benchmark_systems_full(n):
     cfg = synth.config(n)
