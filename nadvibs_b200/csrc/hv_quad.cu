@@ -102,7 +102,7 @@ __device__ __forceinline__ int item_row(int kind, int s) {
 }
 
 template <typename T, int S, int NF>
-__global__ void __launch_bounds__(QUAD_MAXTH, 1)
+__global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
     k_hv_quad(const QuadArgs<T> A, const T *__restrict__ x, T *__restrict__ y, const double *__restrict__ scale_dev,
               double *__restrict__ alpha_part) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -121,6 +121,8 @@ __global__ void __launch_bounds__(QUAD_MAXTH, 1)
     T *s_se = reinterpret_cast<T *>(smem + Lo.se);      // [2][MAXSL][5] slow element factors of a tile
     T *s_dt = reinterpret_cast<T *>(smem + Lo.dt);      // [2][S*S+1] slow diagonal block, energy
     QuadItem *s_it = reinterpret_cast<QuadItem *>(smem + Lo.items);
+    int *s_flag = reinterpret_cast<int *>(smem + Lo.flag);  // [2][nitems]
+    T *s_rec = reinterpret_cast<T *>(smem + Lo.rec);        // [2][nitems][NF+1]
     int *s_ib = reinterpret_cast<int *>(smem + Lo.items + A.nitems * (int)sizeof(QuadItem));
     T *s_ring = reinterpret_cast<T *>(smem + Lo.ring);  // [NS][sst]
     T *s_z = reinterpret_cast<T *>(smem + Lo.z);        // [NF-1][sst] Z_l, l > m
@@ -167,51 +169,72 @@ __global__ void __launch_bounds__(QUAD_MAXTH, 1)
 
     if (tid >= nc) {
         // ---------------- producer ----------------
-        if (tid == nc) {
-            const unsigned bytes = (unsigned)TF * (unsigned)sizeof(T);
-            const int nit = s_ib[S];
-            int slot = 0;
-            unsigned ph = 0;
-            long long issued = 0;
-            bool stop = false;
-            for (int tile = blockIdx.x; tile < A.ntiles && !stop; tile += gridDim.x)
-                for (int it = 0; it < nit; ++it) {
+        // Per tile the warp evaluates which items exist (one bit per item, 32 items per
+        // ballot, word w kept by lane w); lane 0 then issues the copies in item order.
+        const int lane = tid - nc;
+        const unsigned bytes = (unsigned)TF * (unsigned)sizeof(T);
+        const int nit = s_ib[S];
+        const int nw = (nit + 31) >> 5;  // <= 32 words: nitems <= 1024
+        int slot = 0;
+        unsigned ph = 0;
+        long long issued = 0;
+        int stop = 0;
+        for (int tile = blockIdx.x; tile < A.ntiles && !stop; tile += gridDim.x) {
+            unsigned myw = 0;
+            for (int w = 0; w < nw; ++w) {
+                const int it = (w << 5) + lane;
+                bool ok = false;
+                if (it < nit) {
                     const QuadItem q = s_it[it];
+                    ok = true;
                     if (q.kind != QI_OWN) {
                         const int dk = (tile / tsh[q.k]) % snf[q.k];
-                        bool ok = s_tab[(q.k * 5 + item_row(q.kind, q.sk)) * nmax + dk] != (T)0;
+                        ok = s_tab[(q.k * 5 + item_row(q.kind, q.sk)) * nmax + dk] != (T)0;
                         if (q.kind == QI_PAIR) {
                             const int dl = (tile / tsh[q.l]) % snf[q.l];
                             ok = ok && s_tab[(q.l * 5 + item_row(q.kind, q.sl)) * nmax + dl] != (T)0;
                         }
-                        if (!ok) continue;
                     }
-                    if (!mbar_wait(&empty[slot], ph ^ 1u, abort_flag)) {
-                        stop = true;
-                        break;
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                if (lane == w) myw = bal;
+            }
+            const long long tb = (long long)tile * TF;
+            for (int w = 0; w < nw; ++w) {
+                unsigned bits = __shfl_sync(0xffffffffu, myw, w);
+                while (bits) {
+                    const int it = (w << 5) + __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    if (lane == 0 && !stop) {
+                        const QuadItem q = s_it[it];
+                        if (mbar_wait(&empty[slot], ph ^ 1u, abort_flag)) {
+                            mbar_expect_tx(&full[slot], bytes);
+                            bulk_g2s(s_ring + slot * sst + pad, x + q.b * N + tb + (long long)q.tshift * TF, bytes,
+                                     &full[slot]);
+                            ++issued;
+                        } else {
+                            stop = 1;
+                        }
                     }
-                    fence_proxy_async();
-                    mbar_expect_tx(&full[slot], bytes);
-                    bulk_g2s(s_ring + slot * sst + pad, x + q.b * N + (long long)(tile + q.tshift) * TF, bytes,
-                             &full[slot]);
-                    ++issued;
                     if (++slot == NS) {
                         slot = 0;
                         ph ^= 1u;
                     }
                 }
-            if (stop) {
-                // the copies still in flight complete on their full barriers: wait for them
-                // (bounded) before the CTA leaves
-                const long long n = issued < NS ? issued : NS;
-                for (long long i = issued - n; i < issued; ++i) {
-                    const int s = (int)(i % NS);
-                    const unsigned p = (unsigned)((i / NS) & 1);
-                    for (int w = 0; w < WAIT_LIMIT && !mbar_try(&full[s], p); ++w) {
-                    }
-                }
-                atomicExch(A.err, 1);
             }
+            stop = __shfl_sync(0xffffffffu, stop, 0);
+        }
+        if (lane == 0 && stop) {
+            // the copies still in flight complete on their full barriers: wait for them
+            // (bounded) before the CTA leaves
+            const long long n = issued < NS ? issued : NS;
+            for (long long i = issued - n; i < issued; ++i) {
+                const int s2 = (int)(i % NS);
+                const unsigned p = (unsigned)((i / NS) & 1);
+                for (int w = 0; w < WAIT_LIMIT && !mbar_try(&full[s2], p); ++w) {
+                }
+            }
+            atomicExch(A.err, 1);
         }
         return;
     }
@@ -263,6 +286,51 @@ __global__ void __launch_bounds__(QUAD_MAXTH, 1)
         consumer_sync(nc);
         const T *se = s_se + tp * QUAD_MAXSL * 5;
         const T *dt = s_dt + tp * (SS + 1);
+        // item records of the tile: flag (0 absent, 1 neighbour, 2 neighbour feeding Z,
+        // 3 own tile, 4 another state's own tile) and coefficients c, z[j] with the slow
+        // element factors folded in
+        {
+            int *fl = s_flag + tp * A.nitems;
+            T *rc = s_rec + tp * A.nitems * (NF + 1);
+            for (int i = tid; i < A.nitems; i += nc) {
+                const QuadItem q = s_it[i];
+                const int a = q.a, b = q.b;
+                int f;
+                T c = (T)0, z[NF];
+#pragma unroll
+                for (int j = 0; j < NF; ++j) z[j] = (T)0;
+                if (q.kind == QI_OWN) {
+                    f = b == a ? 3 : 4;
+                } else {
+                    T e = se[q.k * 5 + item_row(q.kind, q.sk)];
+                    if (q.kind == QI_PAIR) e *= se[q.l * 5 + item_row(q.kind, q.sl)];
+                    f = e != (T)0 ? 1 : 0;
+                    if (q.kind == QI_SLOW1) {
+                        c = s_G[q.k * SS + a * S + b] * e;
+                        if (b == a) {
+                            bool any = false;
+#pragma unroll
+                            for (int j = 0; j < NF; ++j) {
+                                z[j] = s_Q[(q.k * M + m + j) * S + a] * e;
+                                any |= z[j] != (T)0;
+                            }
+                            if (any && f) f = 2;
+                        }
+                    } else if (q.kind == QI_SLOW2) {
+                        c = s_R[q.k * SS + a * S + b] * e;
+                    } else {
+                        c = s_Q[(q.k * M + q.l) * S + a] * e;
+                    }
+                }
+                fl[i] = f;
+                rc[i * (NF + 1)] = c;
+#pragma unroll
+                for (int j = 0; j < NF; ++j) rc[i * (NF + 1) + 1 + j] = z[j];
+            }
+        }
+        consumer_sync(nc);
+        const int *fl = s_flag + tp * A.nitems;
+        const T *rc = s_rec + tp * A.nitems * (NF + 1);
         const long long tbase = (long long)tile * TF;
 #pragma unroll
         for (int a = 0; a < S; ++a) {
@@ -278,18 +346,27 @@ __global__ void __launch_bounds__(QUAD_MAXTH, 1)
             for (int j = 0; j < NF; ++j) hj[j] = (T)dj[j] + (T)0.5;
             const int iend = s_ib[a + 1];
             for (int it = s_ib[a]; it < iend; ++it) {
-                const QuadItem q = s_it[it];
-                T e = (T)1;
-                if (q.kind != QI_OWN) {
-                    e = se[q.k * 5 + item_row(q.kind, q.sk)];
-                    if (q.kind == QI_PAIR) e *= se[q.l * 5 + item_row(q.kind, q.sl)];
-                    if (e == (T)0) continue;
-                }
-                const bool ok = mbar_wait(&full[slot], ph, abort_flag);
+                const int f = fl[it];
+                if (f == 0) continue;
+                const bool ok = mbar_try(&full[slot], ph) || mbar_wait(&full[slot], ph, abort_flag);
                 const T *buf = s_ring + slot * sst + pad;
                 if (ok) {
-                    const int b = q.b;
-                    if (q.kind == QI_OWN && b == a) {
+                    if (f <= 2) {
+                        T v[R];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) v[r] = buf[r * nc + tid];
+                        const T c = rc[it * (NF + 1)];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) acc[r] += c * v[r];
+                        if (f == 2) {
+#pragma unroll
+                            for (int j = 0; j < NF; ++j) {
+                                const T zq = rc[it * (NF + 1) + 1 + j];
+#pragma unroll
+                                for (int r = 0; r < R; ++r) Z[j][r] += zq * v[r];
+                            }
+                        }
+                    } else if (f == 3) {
 #pragma unroll
                         for (int r = 0; r < R; ++r) xr[r] = buf[r * nc + tid];
                         // diagonal section
@@ -364,8 +441,9 @@ __global__ void __launch_bounds__(QUAD_MAXTH, 1)
                                 acc[r] += rr * v;
                             }
                         }
-                    } else if (q.kind == QI_OWN) {
+                    } else {
                         // another state's own tile
+                        const int b = s_it[it].b;
                         T xb[R];
 #pragma unroll
                         for (int r = 0; r < R; ++r) xb[r] = buf[r * nc + tid];
@@ -402,29 +480,6 @@ __global__ void __launch_bounds__(QUAD_MAXTH, 1)
                                         v = e2p * p[2 * F.sh[j]] + e2m * p[-2 * F.sh[j]];
                                     }
                                     acc[r] += rr * v;
-                                }
-                            }
-                        }
-                    } else {
-                        T v[R];
-#pragma unroll
-                        for (int r = 0; r < R; ++r) v[r] = buf[r * nc + tid];
-                        T c;
-                        if (q.kind == QI_SLOW1) c = s_G[q.k * SS + a * S + b];
-                        else if (q.kind == QI_SLOW2) c = s_R[q.k * SS + a * S + b];
-                        else c = s_Q[(q.k * M + q.l) * S + a];
-                        c *= e;
-                        if (c != (T)0) {
-#pragma unroll
-                            for (int r = 0; r < R; ++r) acc[r] += c * v[r];
-                        }
-                        if (q.kind == QI_SLOW1 && b == a) {
-#pragma unroll
-                            for (int j = 0; j < NF; ++j) {
-                                const T qz = s_Q[(q.k * M + m + j) * S + a] * e;
-                                if (qz != (T)0) {
-#pragma unroll
-                                    for (int r = 0; r < R; ++r) Z[j][r] += qz * v[r];
                                 }
                             }
                         }

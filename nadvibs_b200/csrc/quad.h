@@ -52,7 +52,8 @@ struct QuadItem {
     signed char b;      // source state
     signed char k, sk;  // slow mode and its shift (+-1 or +-2); unused for QI_OWN
     signed char l, sl;  // second slow mode of a bilinear neighbour (QI_PAIR)
-    signed char pad0, pad1;
+    signed char a;      // target state whose list holds the item
+    signed char pad0;
     int tshift;         // sum of the shifts times the slow tile strides
 };
 
@@ -90,7 +91,7 @@ struct QuadPlan {
 
 // Shared-memory layout (byte offsets), identical on host and device.
 struct QuadLayout {
-    int tab, G, R, Q, cst, om, sd, se, dt, items, ring, z, total;
+    int tab, G, R, Q, cst, om, sd, se, dt, items, flag, rec, ring, z, total;
 };
 constexpr int QUAD_MAXSLOT = 16;
 __host__ __device__ inline QuadLayout quad_layout(int M, int S, int nmax, int m, int nF, int sstate, int eb,
@@ -112,6 +113,8 @@ __host__ __device__ inline QuadLayout quad_layout(int M, int S, int nmax, int m,
     L.se = take(2 * QUAD_MAXSL * 5 * eb);
     L.dt = take(2 * (S * S + 1) * eb);
     L.items = take(nitems * (int)sizeof(QuadItem) + (S + 1) * 4);
+    L.flag = take(2 * nitems * 4);                  // per tile parity: item flags
+    L.rec = take(2 * nitems * (nF + 1) * eb);       // per tile parity: c, z[nF] of each item
     o = (o + 127) / 128 * 128;
     L.ring = take(nslot * sstate * eb);
     L.z = take((nF > 1 ? nF - 1 : 1) * sstate * eb);

@@ -125,6 +125,7 @@ bool quad_build(QuadPlan &qp, const Plan &pl, const System &sys) {
         auto push = [&](int kind, int b, int k, int sk, int l, int sl) {
             QuadItem it{};
             it.kind = (signed char)kind;
+            it.a = (signed char)a;
             it.b = (signed char)b;
             it.k = (signed char)k;
             it.sk = (signed char)sk;
@@ -171,12 +172,15 @@ bool quad_build(QuadPlan &qp, const Plan &pl, const System &sys) {
                         for (int sl : {+1, -1}) push(QI_PAIR, a, k, sk, l, sl);
     }
     qp.item_beg[S] = (int)qp.items.size();
+    if (qp.items.size() > 1024) return false;  // the producer keeps one validity bit per item in a warp
     // ring depth: as many slots as fit next to the tables and Z (<= QUAD_MAXSLOT)
     for (int eb : {8, 4}) {
         const int i = eb == 8 ? 0 : 1;
         const size_t fixed = (size_t)quad_layout(M, S, nmax, m, qp.nF, qp.sstate, eb, 0, (int)qp.items.size()).total;
         const size_t slot = (size_t)qp.sstate * eb;
-        const size_t budget = 226 * 1024;
+        // FP64: one CTA per multiprocessor; FP32: two where they fit (more warps to hide latency)
+        size_t budget = eb == 8 ? 226 * 1024 : 112 * 1024;
+        if (fixed + 4 * slot > budget) budget = 226 * 1024;
         if (fixed + 3 * slot > budget) return false;
         qp.nslot[i] = (int)std::min<size_t>(QUAD_MAXSLOT, (budget - fixed) / slot);
         qp.smem[i] = (size_t)quad_layout(M, S, nmax, m, qp.nF, qp.sstate, eb, qp.nslot[i], (int)qp.items.size()).total;
