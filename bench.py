@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--hv-only", action="store_true", help="run H.v launches only (profiling)")
     ap.add_argument("--config", type=int, default=CONFIG_NUMBER)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--basis", type=str, default=None,
+                    help="comma-separated basis overriding the config's (same coefficients; profiling of "
+                         "reduced sizes)")
     return ap.parse_args()
 
 
@@ -116,9 +119,14 @@ def traffic_for(kernel: str, precision: str):
     return d.get(f"{kernel}:{precision}")
 
 
-def make_inputs(cfgn: int, tmpdir: str):
+def make_inputs(cfgn: int, tmpdir: str, basis: str | None = None):
     from nadvibs_b200 import synth
     cfg = synth.config(cfgn)
+    if basis:
+        b = [int(v) for v in basis.split(",")]
+        if len(b) != cfg.nmodes:
+            raise SystemExit(f"--basis needs {cfg.nmodes} values")
+        cfg.basis = b
     return cfg, synth.write_inputs(tmpdir, cfg)
 
 
@@ -128,7 +136,7 @@ def run_ours(args, rank, world, dev):
 
     torch.cuda.set_device(dev)
     tmp = tempfile.mkdtemp(prefix=f"nvb_bench_{rank}_")
-    cfg, (basis, nadvibs) = make_inputs(args.config, tmp)
+    cfg, (basis, nadvibs) = make_inputs(args.config, tmp, args.basis)
     N = cfg.dimen * cfg.nstates
     from nadvibs_b200 import replicas
     results = {}
@@ -140,6 +148,7 @@ def run_ours(args, rank, world, dev):
         pflag = L.NVB_FP64 if prec == "fp64" else L.NVB_MIXED
         eb = 8 if prec == "fp64" else 4
         h = L.Handle.from_files(basis, nadvibs, device=dev, precision=pflag)
+        kname = h.hv_kernel(L.DTYPE_F64 if prec == "fp64" else L.DTYPE_F32)
         st = torch.cuda.Stream(device=dev)
         h.set_stream(st.cuda_stream)
         if args.hv_only:
@@ -174,7 +183,7 @@ def run_ours(args, rank, world, dev):
         hv_ms, it_ms, n = h.timing()
         results[prec] = dict(ms=ms_max, hv_ms_per=hv_ms / max(n, 1), it_ms_per=it_ms / max(n, 1),
                              clocks=clk.summary(), bytes_hv=2 * N * eb, alpha=a[-3:].tolist(),
-                             beta=b[-3:].tolist(), launches=4 * args.steps)
+                             beta=b[-3:].tolist(), launches=4 * args.steps, kernel=kname)
         h.close()
         torch.cuda.empty_cache()
     # end-to-end through the public API with host buffers: create from files (host input),
@@ -257,7 +266,7 @@ def main():
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "cache": "inputs larger than L2 (2.1 GB FP64 vectors), no flush"},
         "roofline": {"bound": "hbm", "achieved": hv_gbs, "peak": peak, "unit": "GB/s", "frac": hv_gbs / peak,
-                     "traffic": traffic_for("hv_slab", main_prec), "kernel": "H.v (k_hv_slab)",
+                     "traffic": traffic_for("hv_" + r["kernel"], main_prec), "kernel": f"H.v (k_hv_{r['kernel']})",
                      "algorithmic_bytes": r["bytes_hv"], "peak_kind": peak_kind},
         "clocks": r["clocks"], "gpu_launches": r["launches"], "e2e": e2e,
     }
@@ -266,7 +275,8 @@ def main():
         mixed_rate = world * args.steps / (m["ms"] / 1e3)
         line["mixed"] = {"value": mixed_rate, "unit": "iter/s", "ratio_vs_fp64": mixed_rate / value,
                          "hv_ms": m["hv_ms_per"], "hv_gbs": m["bytes_hv"] / (m["hv_ms_per"] / 1e3) / 1e9,
-                         "hv_frac": m["bytes_hv"] / (m["hv_ms_per"] / 1e3) / 1e9 / peak}
+                         "hv_frac": m["bytes_hv"] / (m["hv_ms_per"] / 1e3) / 1e9 / peak,
+                         "hv_traffic": traffic_for("hv_" + m["kernel"], "mixed"), "kernel": f"k_hv_{m['kernel']}"}
         line["fp64_hv_ms"] = r["hv_ms_per"]
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(args.config, 1)

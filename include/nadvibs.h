@@ -105,6 +105,11 @@ const char *nvb_last_error(void);
 int nvb_get_sizes(nvb_handle *h, int64_t *dimen, int64_t *nstates, int64_t *nmodes, int64_t *nterms,
                   int64_t *npot, int64_t *iters);
 
+/* Which H.v kernel a product with vectors of this dtype runs (16-byte aligned vectors):
+ * 1 = gather, 2 = slab-tiled, 3 = factorised quadratic.  No reference counterpart (the
+ * reference has one product routine, Source/top.f90:672-818). */
+int nvb_hv_kernel_in_use(nvb_handle *h, int64_t dtype, int64_t *kernel);
+
 /* The merged term table in the reference's representation (nzindx/nzblks/nzcoef of
  * Source/top.f90:199-231): for term t, tcnt[t] distinct modes, tmode[t*4+l] (1-based) and
  * tpow[t*4+l]; tnpair[t] state pairs tpa/tpb[t*nstates^2+q] (1-based) with coefficient

@@ -51,6 +51,7 @@ _SIGS = {
     "nvb_create": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_destroy": [C.c_void_p],
     "nvb_get_sizes": [C.c_void_p] + [C.c_void_p] * 6,
+    "nvb_hv_kernel_in_use": [C.c_void_p, C.c_int64, C.c_void_p],
     "nvb_get_terms": [C.c_void_p] + [C.c_void_p] * 7,
     "nvb_set_precision": [C.c_void_p, C.c_int64],
     "nvb_set_stream": [C.c_void_p, C.c_void_p],
@@ -174,6 +175,12 @@ class Handle:
         v = [C.c_int64() for _ in range(6)]
         check(lib().nvb_get_sizes(self.ptr, *[C.byref(x) for x in v]))
         return dict(zip(("dimen", "nstates", "nmodes", "nterms", "npot", "iters"), [x.value for x in v]))
+
+    def hv_kernel(self, dtype: int = DTYPE_F64) -> str:
+        """Name of the H.v kernel products of this dtype run: gather, slab or quad."""
+        k = C.c_int64()
+        check(lib().nvb_hv_kernel_in_use(self.ptr, dtype, C.byref(k)))
+        return {1: "gather", 2: "slab", 3: "quad"}[k.value]
 
     def terms(self):
         sz = self.sizes()

@@ -191,6 +191,17 @@ int nvb_destroy(nvb_handle *h) {
 
 const char *nvb_last_error(void) { return g_err.c_str(); }
 
+int nvb_hv_kernel_in_use(nvb_handle *h, int64_t dtype, int64_t *kernel) {
+    return guarded([&] {
+        if (!h || !kernel) fail(NVB_ERR_ARG, "null argument");
+        if (dtype != NVB_DTYPE_F64 && dtype != NVB_DTYPE_F32) fail(NVB_ERR_ARG, "dtype must be NVB_DTYPE_F64 or NVB_DTYPE_F32");
+        if (h->device < 0) fail(NVB_ERR_STATE, "host-only handle");
+        if (h->quad.ok) *kernel = 3;
+        else if (h->slab[dtype == NVB_DTYPE_F32 ? 1 : 0].ok) *kernel = 2;
+        else *kernel = 1;
+    });
+}
+
 int nvb_get_sizes(nvb_handle *h, int64_t *dimen, int64_t *nstates, int64_t *nmodes, int64_t *nterms, int64_t *npot,
                   int64_t *iters) {
     return guarded([&] {
