@@ -206,6 +206,23 @@ int nvb_hv_adjoint_coeffs(nvb_handle *h, const void *u, const void *v, int64_t d
  * Exact derivatives for converged roots. */
 int nvb_hellmann_feynman(nvb_handle *h, int64_t nroots, double *grad, double *energies);
 
+/* Record checkpoints of the forward for nvb_lanczos_backward: from the next nvb_seed on,
+ * nvb_lanczos saves (v_{c-1}, v_c) at iterations c = 1, 1+k, 1+2k, ... in device memory
+ * (2 ceil(niter/k) vectors of the handle's precision).  k = 0 stops recording and frees them.
+ * No reference counterpart. */
+int nvb_set_checkpoints(nvb_handle *h, int64_t k);
+
+/* Reverse sweep through the first n Lanczos iterations (plain Lanczos, reorthog = 0): given
+ * alpha_bar[i-1] = dL/dalpha_i and beta_bar[i-1] = dL/dbeta_i (i = 1..n; beta_bar may be NULL
+ * for zeros) of a loss L of T_n, returns grad[ncoef] = dL/dtheta in the layout of
+ * nvb_hv_adjoint_coeffs.  Primal vectors are recomputed segment by segment from checkpoints
+ * every k iterations (the forward's, when nvb_set_checkpoints(h, k) preceded nvb_seed; else one
+ * replay from the seed records them); adjoint vectors and dot products are FP64.  Needs
+ * H^T = H (fails with NVB_ERR_STATE under quirk_lower with inter-state constant or even-power
+ * couplings).  No reference counterpart (the reference has no derivative code). */
+int nvb_lanczos_backward(nvb_handle *h, int64_t n, const double *alpha_bar, const double *beta_bar, int64_t k,
+                         double *grad);
+
 /* <sa*a, sb*b> over the handle's total vector length (dimen*nstates) of two device vectors of
  * dtype, summed in FP64 in a fixed order (block partials in the handle's scratch, then one
  * block); the result is returned in host memory (the call synchronises the stream).

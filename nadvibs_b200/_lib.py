@@ -52,6 +52,8 @@ _SIGS = {
     "nvb_destroy": [C.c_void_p],
     "nvb_get_sizes": [C.c_void_p] + [C.c_void_p] * 6,
     "nvb_hv_kernel_in_use": [C.c_void_p, C.c_int64, C.c_void_p],
+    "nvb_set_checkpoints": [C.c_void_p, C.c_int64],
+    "nvb_lanczos_backward": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p],
     "nvb_get_terms": [C.c_void_p] + [C.c_void_p] * 7,
     "nvb_set_precision": [C.c_void_p, C.c_int64],
     "nvb_set_stream": [C.c_void_p, C.c_void_p],
@@ -291,6 +293,22 @@ class Handle:
     def adjoint_ptr(self, u_ptr: int, v_ptr: int, dtype: int) -> np.ndarray:
         g = np.zeros(self.ncoef())
         check(lib().nvb_hv_adjoint_coeffs(self.ptr, C.c_void_p(u_ptr), C.c_void_p(v_ptr), dtype, _p(g)))
+        return g
+
+    def set_checkpoints(self, k: int):
+        """Record (v_{c-1}, v_c) every k iterations from the next seed (nvb_set_checkpoints)."""
+        check(lib().nvb_set_checkpoints(self.ptr, k))
+
+    def lanczos_backward(self, n: int, alpha_bar, beta_bar=None, k: int = 50) -> np.ndarray:
+        """dL/dtheta from dL/dalpha_1..n and dL/dbeta_1..n (nvb_lanczos_backward)."""
+        ab = np.ascontiguousarray(alpha_bar, dtype=np.float64)
+        if ab.shape != (n,):
+            raise ValueError("alpha_bar must have n entries")
+        bb = None if beta_bar is None else np.ascontiguousarray(beta_bar, dtype=np.float64)
+        if bb is not None and bb.shape != (n,):
+            raise ValueError("beta_bar must have n entries")
+        g = np.zeros(self.ncoef())
+        check(lib().nvb_lanczos_backward(self.ptr, n, _p(ab), None if bb is None else _p(bb), k, _p(g)))
         return g
 
     def hellmann_feynman(self, nroots: int):

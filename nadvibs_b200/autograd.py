@@ -1,0 +1,122 @@
+"""Gradients of Lanczos Ritz energies, Franck-Condon intensities and convolved spectra with
+respect to the Hamiltonian's inputs (no counterpart in the reference, which has no derivative
+code).
+
+``theta`` is the flat vector of ``nadvibs.in`` inputs in the layout of
+``nvb_hv_adjoint_coeffs``: the expansion coefficients (file layout [block][order][monomial],
+file units), the block constants, then the frequencies (hartree).
+
+Forward: a handle is built from ``theta`` (``nvb_create``), seeded as the reference seeds
+(``Source/secondary.f90:727-783``), run for ``niter`` plain Lanczos iterations with
+checkpoints every ``k`` iterations, and T_n = tridiag(beta, alpha, beta) is diagonalised:
+Ritz energies E_i (hartree) and intensities I_i = s_{1,i}^2 (the squared first component of
+eigenvector i, the Franck-Condon weight of the seed, ``Source/secondary.f90:240-257``).
+
+Backward: the eigen-derivatives of the symmetric tridiagonal give dL/dalpha_i and
+dL/dbeta_i,
+    Tbar = S (diag(Ebar) + F o (S^T Sbar)) S^T,   F_ij = 1/(E_j - E_i) (i != j),
+with Sbar = e_1 (2 s_1 Ibar)^T; pairs of nearly equal Ritz values (ghost copies of a
+converged root) are damped, F_ij = d/(d^2 + eps^2).  Then ``nvb_lanczos_backward`` runs the
+reverse sweep through the recurrence on the GPU (segments recomputed from the checkpoints)
+and contracts the adjoint vectors with dH/dtheta.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+from scipy.linalg import eigh_tridiagonal
+
+from . import _lib as L
+
+AU2WAVE = 219474.6313705  # Source/progdata.f90:7
+
+
+def split_theta(theta: np.ndarray, nstates: int, nmodes: int):
+    """(potterms, concoef, omega) views of a flat theta."""
+    nb = nstates * (nstates + 1) // 2
+    npot = theta.size - nb - nmodes
+    if npot < 0:
+        raise ValueError("theta is shorter than concoef + omega")
+    return theta[:npot], theta[npot:npot + nb], theta[npot + nb:]
+
+
+def tridiag_eigh(alpha: np.ndarray, beta_off: np.ndarray):
+    """All eigenpairs of the symmetric tridiagonal T (ascending), LAPACK."""
+    return eigh_tridiagonal(alpha, beta_off)
+
+
+def tridiag_eig_backward(E: np.ndarray, S: np.ndarray, gE: np.ndarray | None, gI: np.ndarray | None,
+                         eps_rel: float = 1e-10):
+    """dL/dalpha (n) and dL/dbeta_1..n-1 (n-1) from dL/dE and dL/dI, I_i = S[0, i]^2."""
+    n = E.size
+    inner = np.zeros((n, n))
+    if gE is not None:
+        inner[np.diag_indices(n)] += gE
+    if gI is not None:
+        sbar0 = 2.0 * S[0, :] * gI                     # Sbar[0, i]; other rows of Sbar are zero
+        ssb = np.outer(S[0, :], sbar0)                 # (S^T Sbar)[j, i] = S[0, j] Sbar[0, i]
+        d = E[None, :] - E[:, None]                    # d[i, j] = E_j - E_i
+        eps = eps_rel * max(1.0, float(np.abs(E).max()))
+        F = d / (d * d + eps * eps)
+        np.fill_diagonal(F, 0.0)
+        inner += F * ssb
+    Tb = S @ inner @ S.T
+    Tb = 0.5 * (Tb + Tb.T)
+    abar = np.diag(Tb).copy()
+    bbar = 2.0 * np.diag(Tb, 1)
+    return abar, bbar
+
+
+class LanczosRitz(torch.autograd.Function):
+    """(E, I) = Ritz energies and intensities of niter Lanczos steps on H(theta)."""
+
+    @staticmethod
+    def forward(ctx, theta: torch.Tensor, params, niter: int, k: int, opts: dict):
+        th = theta.detach().to("cpu", torch.float64).numpy().copy()
+        pot, cc, om = split_theta(th, int(params.nstates), int(params.nmodes))
+        h = L.Handle.from_arrays(params, om, cc, pot, **opts)
+        try:
+            h.set_checkpoints(k)
+            h.seed()
+            a, b = h.lanczos(niter)
+        except Exception:
+            h.close()
+            raise
+        E, S = tridiag_eigh(a[:niter], b[1:niter])
+        ctx.h, ctx.niter, ctx.k = h, niter, k
+        ctx.E, ctx.S = E, S
+        ctx.dev = theta.device
+        out_E = torch.from_numpy(E.copy()).to(theta.device)
+        out_I = torch.from_numpy((S[0, :] ** 2).copy()).to(theta.device)
+        return out_E, out_I
+
+    @staticmethod
+    def backward(ctx, gE, gI):
+        gEn = None if gE is None else gE.detach().to("cpu", torch.float64).numpy()
+        gIn = None if gI is None else gI.detach().to("cpu", torch.float64).numpy()
+        abar, bbar_off = tridiag_eig_backward(ctx.E, ctx.S, gEn, gIn)
+        n = ctx.niter
+        bbar = np.zeros(n)
+        bbar[: n - 1] = bbar_off  # beta_n does not enter T_n
+        try:
+            g = ctx.h.lanczos_backward(n, abar, bbar, ctx.k)
+        finally:
+            ctx.h.close()
+            ctx.h = None
+        return torch.from_numpy(g).to(ctx.dev), None, None, None, None
+
+
+def ritz(theta: torch.Tensor, params, niter: int, k: int = 50, **opts):
+    """Differentiable Ritz energies (hartree) and intensities of niter Lanczos steps."""
+    return LanczosRitz.apply(theta, params, niter, k, opts)
+
+
+def convolved_spectrum(E: torch.Tensor, I: torch.Tensor, grid_cm: torch.Tensor, sigma_cm: float = 20.0,
+                       origin: str = "lowest") -> torch.Tensor:
+    """Gaussian-broadened stick spectrum on grid_cm (cm^-1): sum_i I_i exp(-(x - e_i)^2 / 2 sigma^2),
+    e_i = (E_i - E_0) in cm^-1 with E_0 the lowest Ritz energy (origin "lowest") or 0 ("absolute")."""
+    e = E * AU2WAVE
+    if origin == "lowest":
+        e = e - e.min()
+    x = grid_cm[:, None] - e[None, :]
+    return (I[None, :] * torch.exp(-0.5 * (x / sigma_cm) ** 2)).sum(dim=1)

@@ -182,6 +182,7 @@ int nvb_destroy(nvb_handle *h) {
             slab_free(h->slab[0]);
             slab_free(h->slab[1]);
             quad_free(h->quad);
+            ckpt_free(h);
             if (h->own_stream) cudaStreamDestroy(h->own_stream);
         }
     });
@@ -422,6 +423,26 @@ int nvb_hv_adjoint_coeffs(nvb_handle *h, const void *u, const void *v, int64_t d
         if (dtype != NVB_DTYPE_F64 && dtype != NVB_DTYPE_F32) fail(NVB_ERR_ARG, "bad dtype");
         ensure_device(h);
         hv_adjoint(h, u, v, (int)dtype, grad);
+    });
+}
+
+int nvb_set_checkpoints(nvb_handle *h, int64_t k) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        if (k < 0) fail(NVB_ERR_ARG, "checkpoint interval < 0");
+        ensure_device(h);
+        if (k != h->ck_k) ckpt_free(h);
+        h->ck_k = k;
+        h->ck_count = 0;
+    });
+}
+
+int nvb_lanczos_backward(nvb_handle *h, int64_t n, const double *alpha_bar, const double *beta_bar, int64_t k,
+                         double *grad) {
+    return guarded([&] {
+        if (!h || !alpha_bar || !grad) fail(NVB_ERR_ARG, "null argument");
+        ensure_device(h);
+        lanczos_backward(h, n, alpha_bar, beta_bar, k, grad);
     });
 }
 

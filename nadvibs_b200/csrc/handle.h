@@ -47,6 +47,11 @@ struct nvb_handle {
     std::vector<cudaEvent_t> ev;  // 3 per iteration of a chunk: start, after H.v, end
     double t_hv_ms = 0.0, t_iter_ms = 0.0;
     int64_t n_timed = 0;
+    // checkpoints of the forward for the reverse sweep: (v_{c-1}, v_c) at iterations
+    // c = 1, 1+k, 1+2k, ... in the handle's precision, and their scales
+    int64_t ck_k = 0, ck_count = 0, ck_cap = 0;
+    void *ck_buf = nullptr;
+    double *ck_scale = nullptr;
     // cached scratch for ad-hoc vectors
     void *tmp = nullptr;
     size_t tmp_bytes = 0;
@@ -74,6 +79,10 @@ void save_restart(nvb_handle *h, const char *dir, const char *vdir);
 void load_restart(nvb_handle *h, const char *dir, const char *vdir);
 void hv_adjoint(nvb_handle *h, const void *u, const void *v, int dtype, double *grad);
 void hellmann_feynman(nvb_handle *h, int64_t nroots, double *grad, double *energies);
+void ckpt_reserve(nvb_handle *h, int64_t total_iters);
+void ckpt_save(nvb_handle *h, int64_t it);
+void ckpt_free(nvb_handle *h);
+void lanczos_backward(nvb_handle *h, int64_t n, const double *abar, const double *bbar, int64_t k, double *grad);
 int64_t ncoef_of(const nvb_handle *h);
 void lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state, int64_t *index, double *c2,
                        int64_t *phase, double *pct, const char *rootinfo);

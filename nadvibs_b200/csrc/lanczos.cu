@@ -293,6 +293,7 @@ void lanczos_seed(nvb_handle *h, const double *weights) {
     h->alpha.assign(1, 0.0);
     h->beta.assign(1, beta0);
     h->iters = 0;
+    h->ck_count = 0;
     h->seeded = true;
     h->arch_n = 0;
     h->firststep = true;
@@ -315,6 +316,7 @@ static void passB_launch(nvb_handle *h, int64_t it, int *blocks) {
 static void lanczos_iter(nvb_handle *h, int64_t it, int slot) {
     const int dt = h->precision == NVB_MIXED ? NVB_DTYPE_F32 : NVB_DTYPE_F64;
     int nb = 0;
+    ckpt_save(h, it);
     archive_push(h, it);
     if (h->timing) CK(cudaEventRecord(h->ev[3 * slot], h->stream));
     hv_any(h, h->buf[h->cur], h->buf[h->work], dt, h->d_scale + h->cur, h->d_part, &nb);
@@ -378,6 +380,7 @@ void lanczos_run(nvb_handle *h, int64_t niter) {
     if (niter < 0) fail(NVB_ERR_ARG, "niter < 0");
     grow_scalars(h, h->iters + niter + 1);
     archive_ensure(h, h->iters + niter);
+    ckpt_reserve(h, h->iters + niter);
     if (h->reorthog > 0) {
         if (h->opt.archive_max < h->iters + niter)
             fail(NVB_ERR_ARG, "re-orthogonalisation needs every Lanczos vector: set archive_max >= " +

@@ -1,0 +1,160 @@
+"""Reverse sweep through the Lanczos recurrence (nvb_lanczos_backward) and the differentiable
+Ritz energies / intensities / convolved spectrum (nadvibs_b200.autograd), against central
+finite differences of the GPU forward, against Hellmann-Feynman for a converged root, and for
+consistency across checkpoint intervals and precisions."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from nadvibs_b200 import _lib as L
+from nadvibs_b200 import synth
+from nadvibs_b200.autograd import (convolved_spectrum, ritz, split_theta, tridiag_eig_backward,
+                                   tridiag_eigh)
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(nstates, basis, ordr):
+    p = L.default_params()
+    p.nstates, p.nmodes, p.ordr, p.niter = nstates, len(basis), ordr, 30
+    for i, b in enumerate(basis):
+        p.basis[i] = b
+    return p
+
+
+def _system(seed, nstates, basis, ordr=2, **kw):
+    cfg = synth.random_small(seed, nstates, basis, ordr, offdiag_even=False, **kw)
+    om, cc, pot = synth.draw_small(cfg)
+    return _params(nstates, basis, ordr), np.concatenate([synth.flatten_pot(pot), cc, om])
+
+
+def _forward(p, theta, n, **opts):
+    pot, cc, om = split_theta(theta, p.nstates, p.nmodes)
+    with L.Handle.from_arrays(p, om, cc, pot, **opts) as h:
+        h.seed()
+        a, b = h.lanczos(n)
+    E, S = tridiag_eigh(a[:n], b[1:n])
+    return E, S[0, :] ** 2
+
+
+def _gradient(p, theta, n, gE, gI, k, record=True, **opts):
+    pot, cc, om = split_theta(theta, p.nstates, p.nmodes)
+    with L.Handle.from_arrays(p, om, cc, pot, **opts) as h:
+        if record:
+            h.set_checkpoints(k)
+        h.seed()
+        a, b = h.lanczos(n)
+        E, S = tridiag_eigh(a[:n], b[1:n])
+        abar, bbar_off = tridiag_eig_backward(E, S, gE, gI)
+        bbar = np.zeros(n)
+        bbar[: n - 1] = bbar_off
+        return h.lanczos_backward(n, abar, bbar, k)
+
+
+def _fd(f, theta, idx, rel=1e-5):
+    out = []
+    for i in idx:
+        h = rel * max(abs(theta[i]), 1e-4)
+        tp, tm = theta.copy(), theta.copy()
+        tp[i] += h
+        tm[i] -= h
+        out.append((f(tp) - f(tm)) / (2 * h))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("seed,nstates,basis,n", [(71, 2, [4, 4, 3], 10), (72, 3, [3, 3, 2, 2], 12),
+                                                  (73, 1, [6, 5], 14)])
+def test_backward_matches_finite_differences(seed, nstates, basis, n):
+    p, theta = _system(seed, nstates, basis)
+    rng = np.random.default_rng(seed)
+    gE, gI = rng.normal(size=n), rng.normal(size=n)
+    g = _gradient(p, theta, n, gE, gI, k=4, quirk_lower=0)
+
+    def f(th):
+        E, I = _forward(p, th, n, quirk_lower=0)
+        return float(gE @ E + gI @ I)
+
+    idx = sorted(set(rng.choice(theta.size, size=min(12, theta.size), replace=False).tolist()) | {theta.size - 1})
+    fd = _fd(f, theta, idx)
+    scale = np.abs(fd).max()
+    assert np.abs(g[idx] - fd).max() <= 2e-6 * scale, (g[idx], fd)
+
+
+def test_checkpoint_interval_and_recording_do_not_change_the_gradient():
+    p, theta = _system(74, 2, [4, 3, 3])
+    n = 13
+    rng = np.random.default_rng(74)
+    gE, gI = rng.normal(size=n), rng.normal(size=n)
+    ref = _gradient(p, theta, n, gE, gI, k=n, quirk_lower=0)
+    scale = np.abs(ref).max()
+    for k, rec in [(1, True), (3, True), (5, False), (13, False)]:
+        g = _gradient(p, theta, n, gE, gI, k=k, record=rec, quirk_lower=0)
+        assert np.abs(g - ref).max() <= 1e-12 * scale, (k, rec)
+
+
+def test_converged_root_matches_hellmann_feynman():
+    nstates, basis = 2, [5, 5, 3]
+    p, theta = _system(75, nstates, basis)
+    n = 60
+    pot, cc, om = split_theta(theta, nstates, len(basis))
+    with L.Handle.from_arrays(p, om, cc, pot, quirk_lower=0) as h:
+        h.set_checkpoints(10)
+        h.seed()
+        a, b = h.lanczos(n)
+        E, S = tridiag_eigh(a[:n], b[1:n])
+        assert abs(b[n] * S[-1, 0]) < 1e-9  # the lowest root has converged
+        gE = np.zeros(n)
+        gE[0] = 1.0
+        abar, bbar_off = tridiag_eig_backward(E, S, gE, None)
+        bbar = np.zeros(n)
+        bbar[: n - 1] = bbar_off
+        g = h.lanczos_backward(n, abar, bbar, 10)
+        e_hf, g_hf = h.hellmann_feynman(1)
+    assert e_hf[0] == pytest.approx(E[0], abs=1e-12)
+    assert np.abs(g - g_hf[0]).max() <= 1e-6 * np.abs(g_hf[0]).max()
+
+
+def test_spectrum_gradient_through_autograd_matches_finite_differences():
+    p, theta = _system(76, 2, [4, 4, 3])
+    n = 10
+    grid = torch.linspace(-500.0, 6000.0, 256, dtype=torch.float64)
+    w = torch.from_numpy(np.random.default_rng(76).normal(size=256))
+
+    def loss_t(th):
+        E, I = ritz(th, p, n, k=3, quirk_lower=0)
+        return (w * convolved_spectrum(E, I, grid, 20.0)).sum()
+
+    th = torch.from_numpy(theta.copy()).requires_grad_(True)
+    loss_t(th).backward()
+    g = th.grad.numpy()
+
+    def f(x):
+        E, I = _forward(p, x, n, quirk_lower=0)
+        return float((w * convolved_spectrum(torch.from_numpy(E), torch.from_numpy(I), grid, 20.0)).sum())
+
+    rng = np.random.default_rng(77)
+    idx = sorted(rng.choice(theta.size, size=10, replace=False).tolist())
+    fd = _fd(f, theta, idx)
+    assert np.abs(g[idx] - fd).max() <= 1e-5 * np.abs(fd).max()
+
+
+def test_mixed_precision_gradient_close_to_fp64():
+    p, theta = _system(78, 2, [4, 4, 3])
+    n = 10
+    rng = np.random.default_rng(78)
+    gE, gI = rng.normal(size=n), rng.normal(size=n)
+    g64 = _gradient(p, theta, n, gE, gI, k=4, quirk_lower=0)
+    g32 = _gradient(p, theta, n, gE, gI, k=4, quirk_lower=0, precision=L.NVB_MIXED)
+    assert np.abs(g32 - g64).max() <= 1e-3 * np.abs(g64).max()
+
+
+def test_backward_refuses_one_sided_couplings():
+    cfg = synth.random_small(79, 2, [3, 3], 2, offdiag_even=True, zero_frac=0.0)
+    om, cc, pot = synth.draw_small(cfg)
+    p = _params(2, [3, 3], 2)
+    with L.Handle.from_arrays(p, om, cc, synth.flatten_pot(pot), quirk_lower=1) as h:
+        h.seed()
+        h.lanczos(5)
+        with pytest.raises(L.NvbError):
+            h.lanczos_backward(5, np.ones(5), None, 2)
