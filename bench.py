@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--hv-only", action="store_true", help="run H.v launches only (profiling)")
     ap.add_argument("--config", type=int, default=CONFIG_NUMBER)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-grad", action="store_true", help="skip the gradient (grad/fwd) measurement")
     ap.add_argument("--basis", type=str, default=None,
                     help="comma-separated basis overriding the config's (same coefficients; profiling of "
                          "reduced sizes)")
@@ -206,6 +207,58 @@ def run_ours(args, rank, world, dev):
     return cfg, N, results, e2e
 
 
+def grad_timing(dev: int):
+    """grad/fwd on the gradient system (config 4): forward = seed + 400 plain Lanczos
+    iterations recording checkpoints every 50; backward = eigen-derivatives of T_400 for a
+    loss (Gaussian-convolved spectrum, sigma 20 cm^-1, 2048 points, plus the lowest 20 Ritz
+    energies) and the reverse sweep (nvb_lanczos_backward).  Host wall times around
+    synchronised calls, best of 3."""
+    import numpy as np
+    import torch
+    from nadvibs_b200 import _lib as L
+    from nadvibs_b200 import synth
+    from nadvibs_b200.autograd import AU2WAVE, convolved_spectrum, tridiag_eig_backward, tridiag_eigh
+    cfg = synth.config(4)
+    om, cc, pot = synth.draw(cfg)
+    potf = synth.flatten_pot(pot)
+    p = L.default_params()
+    p.nstates, p.nmodes, p.ordr, p.niter = cfg.nstates, cfg.nmodes, cfg.ordr, cfg.niter
+    for i, b in enumerate(cfg.basis):
+        p.basis[i] = b
+    n, k = 400, 50
+    grid = torch.linspace(-200.0, 8000.0, 2048, dtype=torch.float64)
+    w = torch.from_numpy(np.random.default_rng(4).normal(size=2048))
+    fwd, bwd = [], []
+    for _ in range(3):
+        h = L.Handle.from_arrays(p, om, cc, potf, device=dev)
+        h.set_checkpoints(k)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h.seed()
+        a, b = h.lanczos(n)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        E, S = tridiag_eigh(a[:n], b[1:n])
+        Et = torch.from_numpy(E).requires_grad_(True)
+        It = torch.from_numpy(S[0] ** 2).requires_grad_(True)
+        ((w * convolved_spectrum(Et, It, grid, 20.0)).sum() + (Et[:20] * AU2WAVE).sum()).backward()
+        abar, boff = tridiag_eig_backward(E, S, Et.grad.numpy(), It.grad.numpy())
+        bbar = np.zeros(n)
+        bbar[: n - 1] = boff
+        h.lanczos_backward(n, abar, bbar, k)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        h.close()
+        fwd.append(t1 - t0)
+        bwd.append(t2 - t1)
+    f, g = min(fwd), min(bwd)
+    return {"workload": "config4: 2 states, basis [14,12,10,8,8,6], 1,290,240 functions, ordr 2, 400 plain "
+                        "Lanczos iterations, checkpoints every 50, FP64",
+            "loss": "Gaussian-convolved spectrum (sigma 20 cm^-1, 2048 points) + lowest 20 Ritz energies",
+            "ncoef": int(len(potf) + len(cc) + len(om)), "fwd_ms": 1e3 * f, "grad_ms": 1e3 * g,
+            "grad_over_fwd": g / f}
+
+
 def cpu_baseline_sample(cfgn: int, iters: int):
     """The oracle's restatement of the reference (one streaming pass per term and shift,
     Source/top.f90:672-818, and lanczos_step) on all host cores, bounded sample."""
@@ -278,6 +331,8 @@ def main():
                          "hv_frac": m["bytes_hv"] / (m["hv_ms_per"] / 1e3) / 1e9 / peak,
                          "hv_traffic": traffic_for("hv_" + m["kernel"], "mixed"), "kernel": f"k_hv_{m['kernel']}"}
         line["fp64_hv_ms"] = r["hv_ms_per"]
+    if rank == 0 and not args.no_grad:
+        line["grad"] = grad_timing(local)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(args.config, 1)
     if rank == 0:
