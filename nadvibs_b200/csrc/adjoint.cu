@@ -165,6 +165,124 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_diag(const long long *__res
     }
 }
 
+// ---- ordr <= 2: every P_m is an entry of a Gram matrix G = A^T B over the rows of a state,
+//   A = [u_a, X_k u_a],  B = [v_b, X_k v_b, x_k^2 v_b, (n_k + 1/2) v_b]
+// (X_k the ladder part <n|x|n+-1> along mode k, x_k^2 the analytic square, both truncated to
+// the basis exactly as H.v applies them):
+//   <u_a|v_b> = G[u_a][v_b],  <u_a|x_k|v_b> = G[u_a][X_k v_b],  <u_a|x_k^2|v_b> = G[u_a][x_k^2 v_b],
+//   <u_a|x_k x_l|v_b> = G[X_k u_a][X_l v_b] (X_k symmetric),  K_k = sum_a G[u_a][(n_k+1/2) v_a].
+// Only G1 = u^T B and G2 = (X u)^T (X v) are needed.  One kernel expands the columns of a
+// tile of rows into shared memory and accumulates both; block partials are summed in a fixed
+// order.
+
+constexpr int GRAM_TR = 64;      // rows per shared-memory tile
+constexpr int GRAM_MAXPER = 8;   // Gram outputs per thread: S*(3M+1)*S + (MS)^2 <= 8*256
+
+// Per block: for each tile of GRAM_TR rows, the expanded columns of those rows go to shared
+// memory (one thread per (row, state)), then every thread accumulates its Gram outputs over
+// the tile.  Outputs o < n1: G1[a][j] = <u_a, B_j>; o >= n1: G2[(k,a)][(l,b)] = <X_k u_a, X_l v_b>.
+template <typename T>
+__global__ void __launch_bounds__(256) k_adj_gram(const T *__restrict__ u, const T *__restrict__ v,
+                                                 const double *__restrict__ etab, int nmax,
+                                                 const int *__restrict__ nfunc, const long long *__restrict__ shft,
+                                                 int M, int S, long long dimen, double *__restrict__ part) {
+    extern __shared__ double sm[];
+    const int MS = M * S, nA = S + MS, nB = S + 3 * MS;
+    const int n1 = S * nB, n2 = MS * MS, nout = n1 + n2;
+    double *sA = sm, *sB = sm + GRAM_TR * nA;  // [row][col]
+    const double *E1 = etab + (0 * ETAB_J + 1) * nmax;  // <m|x|m+1>
+    const double *E2 = etab + (1 * ETAB_J + 2) * nmax;  // <m|x^2|m+2>
+    const double *D2 = etab + (1 * ETAB_J + 0) * nmax;  // <m|x^2|m>
+    const int tid = threadIdx.x, nth = blockDim.x;
+    double acc[GRAM_MAXPER];
+#pragma unroll
+    for (int q = 0; q < GRAM_MAXPER; ++q) acc[q] = 0.0;
+    for (long long t0 = (long long)blockIdx.x * GRAM_TR; t0 < dimen; t0 += (long long)gridDim.x * GRAM_TR) {
+        for (int e = tid; e < GRAM_TR * S; e += nth) {
+            const int rl = e % GRAM_TR, s = e / GRAM_TR;
+            const long long r = t0 + rl;
+            double *a = sA + rl * nA, *b = sB + rl * nB;
+            if (r >= dimen) {
+                a[s] = 0.0;
+                b[s] = 0.0;
+                for (int k = 0; k < M; ++k) {
+                    a[S + k * S + s] = 0.0;
+                    b[S + k * S + s] = b[S + MS + k * S + s] = b[S + 2 * MS + k * S + s] = 0.0;
+                }
+                continue;
+            }
+            const T *us = u + s * dimen, *vs = v + s * dimen;
+            const double u0 = (double)us[r], v0 = (double)vs[r];
+            a[s] = u0;
+            b[s] = v0;
+            long long rem = r;
+            for (int k = 0; k < M; ++k) {
+                const long long sh = shft[k];
+                const int d = (int)(rem / sh);
+                rem -= (long long)d * sh;
+                const int nf = nfunc[k];
+                double xu = 0.0, xv = 0.0, tv = D2[d] * v0;
+                if (d + 1 < nf) {
+                    const double e = E1[d];
+                    xu += e * (double)us[r + sh];
+                    xv += e * (double)vs[r + sh];
+                }
+                if (d >= 1) {
+                    const double e = E1[d - 1];
+                    xu += e * (double)us[r - sh];
+                    xv += e * (double)vs[r - sh];
+                }
+                if (d + 2 < nf) tv += E2[d] * (double)vs[r + 2 * sh];
+                if (d >= 2) tv += E2[d - 2] * (double)vs[r - 2 * sh];
+                a[S + k * S + s] = xu;
+                b[S + k * S + s] = xv;
+                b[S + MS + k * S + s] = tv;
+                b[S + 2 * MS + k * S + s] = ((double)d + 0.5) * v0;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < GRAM_MAXPER; ++q) {
+            const int o = tid + q * nth;
+            if (o < nout) {
+                int ia, jb;
+                if (o < n1) {
+                    ia = o / nB;
+                    jb = o - ia * nB;
+                } else {
+                    const int o2 = o - n1;
+                    ia = S + o2 / MS;
+                    jb = S + (o2 - (o2 / MS) * MS);
+                }
+                double x = acc[q];
+                for (int r = 0; r < GRAM_TR; ++r) x += sA[r * nA + ia] * sB[r * nB + jb];
+                acc[q] = x;
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < GRAM_MAXPER; ++q) {
+        const int o = tid + q * nth;
+        if (o < nout) part[(long long)blockIdx.x * nout + o] = acc[q];
+    }
+}
+
+static bool gram_fits(int S, int M) {
+    const int MS = M * S, nA = S + MS, nB = S + 3 * MS;
+    return S * nB + MS * MS <= GRAM_MAXPER * 256 && (size_t)GRAM_TR * (nA + nB) * sizeof(double) <= 200 * 1024;
+}
+
+// out[o] (+)= sum over blocks g = 0..ng-1 of part[g][o], in block order
+__global__ void k_gram_reduce(const double *__restrict__ part, int ng, int nout, int accumulate,
+                              double *__restrict__ out) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nout) return;
+    double s = 0.0;
+    for (int g = 0; g < ng; ++g) s += part[(long long)g * nout + o];
+    out[o] = accumulate ? out[o] + s : s;
+}
+
 static int smax_of(int p, int64_t nf) {
     int s = p;
     while (s > nf - 1) s -= 2;
@@ -206,6 +324,53 @@ static void launch_chunk(nvb_handle *h, const std::vector<AdjStep> &steps, const
     cudaFree(d);
 }
 
+// P[m][a][b] for the monomials of an ordr <= 2 system and Cq = (C[a][b], K_k), via the Gram matrix.
+template <typename T>
+static void gram_adjoint(nvb_handle *h, const T *u, const T *v, const std::vector<Mono> &monos, std::vector<double> &P,
+                         std::vector<double> &Cq) {
+    const System &sys = h->sys;
+    const Plan &pl = h->plan;
+    const int S = sys.S, M = sys.M;
+    // expanded columns: A = [u (S), X u (M S)], B = [v (S), X v (M S), x^2 v (M S), (n+1/2) v (M S)];
+    // two Grams: G1 = u^T B (S x nB), G2 = (X u)^T (X v) (MS x MS)
+    const int MS = M * S, nA = S + MS, nB = S + 3 * MS;
+    const int n1 = S * nB, n2 = MS * MS, nout = n1 + n2;
+    if (!gram_fits(S, M)) fail(NVB_ERR_ARG, "adjoint: too many modes x states for the Gram path");
+    const long long Ns = sys.dimen;
+    const int grid = (int)std::min<long long>((Ns + GRAM_TR - 1) / GRAM_TR, 148 * 4);
+    double *scr = (double *)scratch_vector(h, ((size_t)grid * nout + nout) * sizeof(double));
+    double *part = scr, *G = scr + (size_t)grid * nout;
+    const size_t shm = (size_t)GRAM_TR * (nA + nB) * sizeof(double);
+    if (shm > 48 * 1024) CK(cudaFuncSetAttribute(k_adj_gram<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    k_adj_gram<T><<<grid, 256, shm, h->stream>>>(u, v, pl.d_etab, pl.nmax, pl.d_nfunc, pl.d_shft, M, S, Ns, part);
+    k_gram_reduce<<<(nout + 255) / 256, 256, 0, h->stream>>>(part, grid, nout, 0, G);
+    CK(cudaGetLastError());
+    std::vector<double> G1h(n1), G2h(n2);
+    CK(cudaMemcpyAsync(G1h.data(), G, n1 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(G2h.data(), G + n1, n2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    auto g = [&](int a, int j) { return G1h[(size_t)a * nB + j]; };            // <u_a, B_j>
+    auto g2 = [&](int k, int a, int l, int b) { return G2h[(size_t)(k * S + a) * MS + l * S + b]; };
+    const int nm = (int)monos.size();
+    P.assign((size_t)nm * S * S, 0.0);
+    for (int t = 0; t < nm; ++t) {
+        const Mono &mo = monos[t];
+        for (int a = 0; a < S; ++a)
+            for (int b = 0; b < S; ++b) {
+                double val = 0.0;
+                if (mo.modes.size() == 1 && mo.pows[0] == 1) val = g(a, S + mo.modes[0] * S + b);
+                else if (mo.modes.size() == 1) val = g(a, S + M * S + mo.modes[0] * S + b);
+                else val = g2(mo.modes[0], a, mo.modes[1], b);
+                P[(size_t)t * S * S + a * S + b] = val;
+            }
+    }
+    Cq.assign((size_t)S * S + M, 0.0);
+    for (int a = 0; a < S; ++a)
+        for (int b = 0; b < S; ++b) Cq[a * S + b] = g(a, b);
+    for (int k = 0; k < M; ++k)
+        for (int a = 0; a < S; ++a) Cq[S * S + k] += g(a, S + 2 * M * S + k * S + a);
+}
+
 template <typename T, int S>
 static void adjoint_s(nvb_handle *h, const T *u, const T *v, double *grad) {
     constexpr int TB = S * S <= 4 ? 8 : (S * S <= 9 ? 3 : 2);
@@ -217,6 +382,10 @@ static void adjoint_s(nvb_handle *h, const T *u, const T *v, double *grad) {
     const int grid = 148 * 4;
     // P[m][a][b]
     std::vector<double> P((size_t)nm * S * S, 0.0);
+    std::vector<double> Cq;
+    if (sys.ordr <= 2 && gram_fits(S, M)) {
+        gram_adjoint<T>(h, u, v, monos, P, Cq);
+    } else {
     double *part = nullptr;
     CK(cudaMalloc((void **)&part, (size_t)grid * std::max(TB * S * S, S * S + M) * sizeof(double)));
     for (int m0 = 0; m0 < nm; m0 += TB) {
@@ -271,9 +440,10 @@ static void adjoint_s(nvb_handle *h, const T *u, const T *v, double *grad) {
     CK(cudaMemcpyAsync(hq.data(), part, hq.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     cudaFree(part);
-    std::vector<double> Cq(nout, 0.0);
+    Cq.assign(nout, 0.0);
     for (int q = 0; q < nout; ++q)
         for (int g = 0; g < grid; ++g) Cq[q] += hq[(size_t)g * nout + q];
+    }
     // assemble
     const int nb = sys.nstblks();
     const int64_t npot = (int64_t)sys.potterms.size();

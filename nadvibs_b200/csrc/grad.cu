@@ -18,9 +18,10 @@
 // The primal vectors come back segment by segment, last segment first: the forward saves
 // (v_{c-1}, v_c) every k iterations (nvb_set_checkpoints), and each segment of k iterations
 // is replayed from its checkpoint with the stored alpha/beta in the handle's precision, the
-// same way the two-pass Ritz vectors are rebuilt.  The segment's vectors are kept in FP64;
-// the adjoint vectors and every dot product are FP64.  Device memory: 2 ceil(n/k) checkpoint
-// vectors (handle precision) + (k + 2) FP64 segment vectors + 6 FP64 work vectors.
+// same way the two-pass Ritz vectors are rebuilt; the replay keeps v_j and w_j = H v_j of the
+// segment in FP64.  The adjoint vectors and every dot product are FP64.  Device memory:
+// 2 ceil(n/k) checkpoint vectors (handle precision) + (2k + 3) FP64 segment vectors + 6 FP64
+// work vectors.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -141,10 +142,10 @@ void ckpt_free(nvb_handle *h) {
 // ---------------------------------------------------------------- replay
 
 // Replays iterations from (prev = v_{c-1}, cur = v_c) in the handle's precision, writing the
-// FP64 vectors v_{c-1} .. v_{last} to seg[0 .. last-c+1].  The three native buffers are
-// scratch; the scales are host values.
+// FP64 vectors v_{c-1} .. v_{last} to seg[0 .. last-c+1] and w_j = H v_j (j = c .. last-1) to
+// wseg[0 .. last-c-1].  The three native buffers are scratch; the scales are host values.
 static void replay_segment(nvb_handle *h, void *b3[3], double sprev, double scur, int64_t c, int64_t last,
-                           double *seg, double *dsc) {
+                           double *seg, double *wseg, double *dsc) {
     const long long N = h->ntotal();
     const bool mixed = h->precision == NVB_MIXED;
     const int dt = mixed ? NVB_DTYPE_F32 : NVB_DTYPE_F64;
@@ -159,6 +160,7 @@ static void replay_segment(nvb_handle *h, void *b3[3], double sprev, double scur
         if (j == last) break;
         CK(cudaMemcpyAsync(dsc, &scur, sizeof(double), cudaMemcpyHostToDevice, h->stream));
         hv_any(h, b3[cur], b3[work], dt, dsc, nullptr, nullptr);
+        to64(wseg + (size_t)(j - c) * N, b3[work], 1.0);  // w_j = H v_j, kept for the sweep
         if (mixed)
             k_replay<float><<<grid_g(N), 256, 0, h->stream>>>((float *)b3[work], (const float *)b3[cur],
                                                               (const float *)b3[prev], scur, sprev, h->alpha[j],
@@ -286,9 +288,10 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
     std::vector<double> cks(2 * (size_t)nseg);
     CK(cudaMemcpy(cks.data(), h->ck_scale, cks.size() * sizeof(double), cudaMemcpyDeviceToHost));
 
-    DevBuf segb((size_t)(k + 2) * per64), b0(per), b1(per), b2(per), dscb(sizeof(double));
+    DevBuf segb((size_t)(k + 2) * per64), wsegb((size_t)(k + 1) * per64), b0(per), b1(per), b2(per),
+        dscb(sizeof(double));
     DevBuf vbn(per64), vbc(per64), vbp(per64), rb(per64), wb(per64), w(per64);
-    double *seg = (double *)segb.p;
+    double *seg = (double *)segb.p, *wseg = (double *)wsegb.p;
     void *b3[3] = {b0.p, b1.p, b2.p};
     double *vb_next = (double *)vbn.p, *vb_cur = (double *)vbc.p, *vb_prev = (double *)vbp.p;
     double *rbar = (double *)rb.p, *wbar = (double *)wb.p, *wv = (double *)w.p;
@@ -308,16 +311,16 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
         CK(cudaMemcpyAsync(b3[0], (char *)h->ck_buf + 2 * (size_t)s * per, per, cudaMemcpyDeviceToDevice, h->stream));
         CK(cudaMemcpyAsync(b3[1], (char *)h->ck_buf + (2 * (size_t)s + 1) * per, per, cudaMemcpyDeviceToDevice,
                            h->stream));
-        replay_segment(h, b3, cks[2 * s], cks[2 * s + 1], c, e + 1, seg, (double *)dscb.p);
+        replay_segment(h, b3, cks[2 * s], cks[2 * s + 1], c, e + 1, seg, wseg, (double *)dscb.p);
         auto V = [&](int64_t j) { return seg + (size_t)(j - (c - 1)) * N; };  // v_j, c-1 <= j <= e+1
         for (int64_t i = e; i >= c; --i) {
             const double al = h->alpha[i], be = h->beta[i], bprev = h->beta[i - 1];
-            hv_any(h, V(i), wv, NVB_DTYPE_F64, nullptr, nullptr, nullptr);  // w_i = H v_i
+            const double *wi = wseg + (size_t)(i - c) * N;  // w_i = H v_i from the replay
             const double btot = bbar[i] - dot(vb_next, V(i + 1)) / be;
             k_lin<<<g, 256, 0, h->stream>>>(rbar, 1.0 / be, vb_next, btot, V(i + 1), 0, N);
             const double atot = abar[i - 1] - dot(rbar, V(i));
             if (i > 1) bbar[i - 1] -= dot(rbar, V(i - 1));
-            k_lin<<<g, 256, 0, h->stream>>>(vb_cur, -al, rbar, atot, wv, 1, N);
+            k_lin<<<g, 256, 0, h->stream>>>(vb_cur, -al, rbar, atot, wi, 1, N);
             k_lin<<<g, 256, 0, h->stream>>>(wbar, 1.0, rbar, atot, V(i), 0, N);
             if (i > 1) k_lin<<<g, 256, 0, h->stream>>>(vb_prev, -bprev, rbar, 0.0, nullptr, 1, N);
             hv_any(h, wbar, wv, NVB_DTYPE_F64, nullptr, nullptr, nullptr);  // H wbar
