@@ -190,6 +190,18 @@ int nvb_load_restart(nvb_handle *h, const char *dir, const char *vecdir);
 int nvb_lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state, int64_t *index, double *c2,
                           int64_t *phase, double *pct, const char *rootinfo_path);
 
+/* Spin-orbit parameters of the lowest soroots Ritz pairs (Source/top.f90:1153-1175 and
+ * 1231-1252, the soroots branch of identify_roots): energy_ev[i] = E_i in eV,
+ * amp[i] = sqrt(I_i / I_max) * sign_i with I_max the largest intensity among the lowest nroots
+ * roots (the reference uses nroots = max(idroots, soroots)) and sign_i the sign of the first
+ * eigenvector component, and overlap[((i*soroots + j)*nstates + k)*nstates + l] =
+ * <psi_i restricted to state k | psi_j restricted to state l> for j < i (zero for j >= i),
+ * from the Ritz vectors (archive or two-pass replay).  sodata_path (optional) receives
+ * sodata.in in the reference's format (its overlap rows only for 2 or 3 states, as the
+ * reference writes them).  Any output array may be NULL. */
+int nvb_spin_orbit(nvb_handle *h, int64_t soroots, int64_t nroots, double *energy_ev, double *amp, double *overlap,
+                   const char *sodata_path);
+
 /* Adjoint contraction of the gradient path (no counterpart in the reference):
  * grad[npot + nstblks + nmodes] = d<u|H(theta)|v>/d theta for theta = (the potterms of
  * nvb_create's layout -- every nadvibs.in expansion coefficient, zero ones included --, the

@@ -53,6 +53,7 @@ _SIGS = {
     "nvb_get_sizes": [C.c_void_p] + [C.c_void_p] * 6,
     "nvb_hv_kernel_in_use": [C.c_void_p, C.c_int64, C.c_void_p],
     "nvb_set_checkpoints": [C.c_void_p, C.c_int64],
+    "nvb_spin_orbit": [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p],
     "nvb_lanczos_backward": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p],
     "nvb_get_terms": [C.c_void_p] + [C.c_void_p] * 7,
     "nvb_set_precision": [C.c_void_p, C.c_int64],
@@ -294,6 +295,17 @@ class Handle:
         g = np.zeros(self.ncoef())
         check(lib().nvb_hv_adjoint_coeffs(self.ptr, C.c_void_p(u_ptr), C.c_void_p(v_ptr), dtype, _p(g)))
         return g
+
+    def spin_orbit(self, soroots: int, nroots: int | None = None, path: str | None = None) -> dict:
+        """nvb_spin_orbit: energies (eV), sqrt(I/Imax)*sign and state-block overlaps of the lowest
+        soroots Ritz vectors; writes sodata.in to path when given."""
+        nroots = soroots if nroots is None else nroots
+        S = self.sizes()["nstates"]
+        e, amp = np.zeros(soroots), np.zeros(soroots)
+        ov = np.zeros((soroots, soroots, S, S))
+        check(lib().nvb_spin_orbit(self.ptr, soroots, nroots, _p(e), _p(amp), _p(ov),
+                                   None if path is None else path.encode()))
+        return dict(energy_ev=e, amp=amp, overlap=ov)
 
     def set_checkpoints(self, k: int):
         """Record (v_{c-1}, v_c) every k iterations from the next seed (nvb_set_checkpoints)."""

@@ -426,6 +426,15 @@ int nvb_hv_adjoint_coeffs(nvb_handle *h, const void *u, const void *v, int64_t d
     });
 }
 
+int nvb_spin_orbit(nvb_handle *h, int64_t soroots, int64_t nroots, double *energy_ev, double *amp, double *overlap,
+                   const char *sodata_path) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        ensure_device(h);
+        spin_orbit(h, soroots, nroots, energy_ev, amp, overlap, sodata_path);
+    });
+}
+
 int nvb_set_checkpoints(nvb_handle *h, int64_t k) {
     return guarded([&] {
         if (!h) fail(NVB_ERR_ARG, "null handle");

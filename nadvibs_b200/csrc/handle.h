@@ -86,4 +86,6 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar, const double
 int64_t ncoef_of(const nvb_handle *h);
 void lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state, int64_t *index, double *c2,
                        int64_t *phase, double *pct, const char *rootinfo);
+void spin_orbit(nvb_handle *h, int64_t soroots, int64_t nroots, double *e_ev, double *amp, double *ov,
+                const char *path);
 }  // namespace nvb

@@ -119,6 +119,27 @@ __global__ void k_state_norms(const double *__restrict__ psi, long long dimen, i
     }
 }
 
+// part[blockIdx.x * S*S + k*S + l] = partial sum of a[k][r] * b[l][r] (state blocks of length dimen)
+__global__ void k_state_cross(const double *__restrict__ a, const double *__restrict__ b, long long dimen, int S,
+                              double *__restrict__ part) {
+    __shared__ double red[256];
+    for (int k = 0; k < S; ++k)
+        for (int l = 0; l < S; ++l) {
+            double acc = 0.0;
+            const long long stride = (long long)gridDim.x * blockDim.x;
+            for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < dimen; i += stride)
+                acc += a[(long long)k * dimen + i] * b[(long long)l * dimen + i];
+            red[threadIdx.x] = acc;
+            __syncthreads();
+            for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+                if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) part[(long long)blockIdx.x * S * S + k * S + l] = red[0];
+            __syncthreads();
+        }
+}
+
 static int grid_n(long long n) {
     long long b = (n + 1023) / 1024;
     if (b > 148 * 8) b = 148 * 8;
@@ -600,6 +621,88 @@ void lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state,
     cudaFree(bval);
     cudaFree(bidx);
     cudaFree(spart);
+}
+
+// Spin-orbit parameters of identify_roots (Source/top.f90:1153-1175,1231-1252): for the lowest
+// soroots Ritz pairs, E_i in eV and sqrt(I_i / I_max) * sign_i (I_max over the lowest nroots,
+// sign_i the sign of the first eigenvector component), and for j < i the overlaps of the state
+// blocks of the Ritz vectors, ov[i][j][k][l] = sum_r psi_i[k][r] psi_j[l][r].  sodata.in gets
+// the reference's text: the overlaps with k != l, in the order (k outer, l inner), for 2 or 3
+// states (the reference writes no overlap rows for other state counts).
+void spin_orbit(nvb_handle *h, int64_t soroots, int64_t nroots, double *e_ev, double *amp, double *ov,
+                const char *path) {
+    const int64_t n = h->iters;
+    if (n < 1) fail(NVB_ERR_STATE, "no Lanczos iterations");
+    if (soroots < 1 || soroots > n) fail(NVB_ERR_ARG, "soroots must be in 1..iterations");
+    if (nroots < soroots || nroots > n) fail(NVB_ERR_ARG, "nroots must be in soroots..iterations");
+    const long long N = h->ntotal();
+    const int S = h->sys.S;
+    std::vector<double> E(n), V((size_t)n * n);
+    tridiag_eigen(n, h->alpha.data() + 1, h->beta.data() + 1, E.data(), V.data());
+    double intfactor = 0.0;
+    for (int64_t i = 0; i < nroots; ++i) intfactor = std::max(intfactor, V[(size_t)i * n] * V[(size_t)i * n]);
+    std::vector<double> ee(soroots), aa(soroots), oo((size_t)soroots * soroots * S * S, 0.0);
+    for (int64_t i = 0; i < soroots; ++i) {
+        const double v1 = V[(size_t)i * n];
+        ee[i] = E[i] * AU2EV;
+        aa[i] = (intfactor > 0 ? std::sqrt(v1 * v1 / intfactor) : 0.0) * (v1 < 0 ? -1.0 : 1.0);
+    }
+    double *psi = nullptr, *part = nullptr;
+    const int nb = grid_n(h->sys.dimen) > 1024 ? 1024 : grid_n(h->sys.dimen);
+    CK(cudaMalloc((void **)&psi, (size_t)soroots * N * sizeof(double)));
+    try {
+        CK(cudaMalloc((void **)&part, (size_t)nb * S * S * sizeof(double)));
+        ritz_vectors(h, soroots, V, psi);
+        std::vector<double> hp((size_t)nb * S * S);
+        for (int64_t i = 1; i < soroots; ++i)
+            for (int64_t j = 0; j < i; ++j) {
+                k_state_cross<<<nb, 256, 0, h->stream>>>(psi + (size_t)i * N, psi + (size_t)j * N, h->sys.dimen, S,
+                                                         part);
+                CK(cudaGetLastError());
+                CK(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+                CK(cudaStreamSynchronize(h->stream));
+                double *dst = oo.data() + ((size_t)i * soroots + j) * S * S;
+                for (int q = 0; q < nb; ++q)
+                    for (int kl = 0; kl < S * S; ++kl) dst[kl] += hp[(size_t)q * S * S + kl];
+            }
+    } catch (...) {
+        cudaFree(psi);
+        if (part) cudaFree(part);
+        throw;
+    }
+    cudaFree(psi);
+    cudaFree(part);
+    if (e_ev) std::copy(ee.begin(), ee.end(), e_ev);
+    if (amp) std::copy(aa.begin(), aa.end(), amp);
+    if (ov) std::copy(oo.begin(), oo.end(), ov);
+    if (path && *path) {
+        FILE *f = std::fopen(path, "w");
+        if (!f) fail(NVB_ERR_IO, std::string("cannot write ") + path);
+        std::fprintf(f, "%s\n", fI(soroots, 5).c_str());
+        std::fprintf(f, " Root   Energy (eV)      Sqrt(Int.)*sign\n");
+        for (int64_t i = 0; i < soroots; ++i)
+            std::fprintf(f, "%s  %s  %s\n", fI(i + 1, 5).c_str(), fES(ee[i], 15, 8).c_str(), fES(aa[i], 15, 8).c_str());
+        if (S == 2) std::fprintf(f, " R(i)  R(j)   [S1(i)S2(j)]   [S2(i)S1(j)]\n");
+        if (S == 3)
+            std::fprintf(f, " R(i)  R(j)   [S1(i)S2(j)]   [S1(i)S3(j)]  [S2(i)S1(j)]\n"
+                            " R(i)  R(j)   [S2(i)S3(j)]   [S3(i)S1(j)]  [S3(i)S2(j)]\n");
+        if (S == 2 || S == 3)
+            for (int64_t i = 1; i < soroots; ++i)
+                for (int64_t j = 0; j < i; ++j) {
+                    const double *o = oo.data() + ((size_t)i * soroots + j) * S * S;
+                    std::vector<double> dp;
+                    for (int k = 0; k < S; ++k)
+                        for (int l = 0; l < S; ++l)
+                            if (k != l) dp.push_back(o[k * S + l]);
+                    const std::string ij = fI(i + 1, 5) + " " + fI(j + 1, 5) + "  ";
+                    if (S == 2) std::fprintf(f, "%s%s %s\n", ij.c_str(), fES(dp[0], 14, 6).c_str(), fES(dp[1], 14, 6).c_str());
+                    else
+                        std::fprintf(f, "%s%s %s %s\n%s%s %s %s\n", ij.c_str(), fES(dp[0], 14, 6).c_str(),
+                                     fES(dp[1], 14, 6).c_str(), fES(dp[2], 14, 6).c_str(), ij.c_str(),
+                                     fES(dp[3], 14, 6).c_str(), fES(dp[4], 14, 6).c_str(), fES(dp[5], 14, 6).c_str());
+                }
+        std::fclose(f);
+    }
 }
 
 }  // namespace nvb

@@ -5,8 +5,8 @@
 
 reads ``basis.in`` and ``nadvibs.in`` from the working directory, and writes ``output.dat``
 (header and eigenvalue table), ``restart.log`` (working directory) with ``nadvibs.35.0``
-(scratch directory), and ``rootinfo.dat`` when ``idroots``/``soroots`` ask for root
-identification.  ``restart != 0`` in basis.in resumes from restart.log / nadvibs.35.0 and
+(scratch directory), ``rootinfo.dat`` when ``idroots``/``soroots`` ask for root
+identification, and ``sodata.in`` (spin-orbit parameters) when ``soroots > 0``.  ``restart != 0`` in basis.in resumes from restart.log / nadvibs.35.0 and
 runs ``niter`` further iterations, as the reference does (Source/secondary.f90:857-861).
 ``-m`` is accepted for compatibility (the reference only prints it).
 """
@@ -81,6 +81,8 @@ def run(workdir: str = ".", outdir: str | None = None, precision: str = "fp64", 
         leads = None
         if nroots > 0:
             leads = h.lead_contributors(nroots, params.idroots, os.path.join(workdir, "rootinfo.dat"))
+        if params.soroots > 0:
+            h.spin_orbit(params.soroots, nroots, os.path.join(workdir, "sodata.in"))
         with open(out, "a") as f:
             f.write(" \nCalculation completed.\n")
         return dict(alpha=a, beta=b, leads=leads, seconds=time.time() - t0)

@@ -82,5 +82,13 @@ module nadvibs_gpu
       real(c_double), dimension(*), intent(out) :: c2, pct
       character(kind=c_char), dimension(*), intent(in) :: rootinfo
     end function
+    integer(c_int) function nvb_spin_orbit(h, soroots, nroots, energy_ev, amp, overlap, sodata) &
+        bind(C, name="nvb_spin_orbit")
+      import :: c_int, c_int64_t, c_double, c_char, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: soroots, nroots
+      real(c_double), dimension(*), intent(out) :: energy_ev, amp, overlap
+      character(kind=c_char), dimension(*), intent(in) :: sodata
+    end function
   end interface
 end module nadvibs_gpu

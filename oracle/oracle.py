@@ -284,6 +284,35 @@ def eigen_table_lines(alpha, beta, omega, bjiconv: float):
     return out
 
 
+def sodata_lines(E, inten, sign, psi, soroots: int, nroots: int, nstates: int):
+    """The text of sodata.in (Source/top.f90:1153-1175, 1231-1252, formats 1001-1005 and
+    1013-1014) from the Ritz values/intensities/signs of T_n and the Ritz vectors psi[i]
+    (flat, state blocks of equal length): root lines, then for i > j the overlaps of state
+    block k of psi_i with state block l of psi_j, k != l, k outer."""
+    fac = max(inten[:nroots])
+    out = [_I(soroots, 5), " Root   Energy (eV)      Sqrt(Int.)*sign"]
+    for i in range(soroots):
+        out.append(_I(i + 1, 5) + "  " + _ES(E[i] * AU2EV, 15, 8) + "  " + _ES(np.sqrt(inten[i] / fac) * sign[i], 15, 8))
+    if nstates == 2:
+        out.append(" R(i)  R(j)   [S1(i)S2(j)]   [S2(i)S1(j)]")
+    if nstates == 3:
+        out += [" R(i)  R(j)   [S1(i)S2(j)]   [S1(i)S3(j)]  [S2(i)S1(j)]",
+                " R(i)  R(j)   [S2(i)S3(j)]   [S3(i)S1(j)]  [S3(i)S2(j)]"]
+    if nstates in (2, 3):
+        for i in range(1, soroots):
+            blk_i = np.asarray(psi[i]).reshape(nstates, -1)
+            for j in range(i):
+                blk_j = np.asarray(psi[j]).reshape(nstates, -1)
+                dp = [float(blk_i[k] @ blk_j[l]) for k in range(nstates) for l in range(nstates) if k != l]
+                head = _I(i + 1, 5) + " " + _I(j + 1, 5) + "  "
+                if nstates == 2:
+                    out.append(head + _ES(dp[0], 14, 6) + " " + _ES(dp[1], 14, 6))
+                else:
+                    out.append(head + " ".join(_ES(x, 14, 6) for x in dp[:3]))
+                    out.append(head + " ".join(_ES(x, 14, 6) for x in dp[3:]))
+    return out
+
+
 def extract_spectrum(path: str, threshold: float = 1e-15):
     """extract.py:22-50: (E_eV, I, convergence) rows of output.dat's table with convergence <
     threshold and I != 0, in table order."""

@@ -126,3 +126,49 @@ def test_lead_contributors_match_oracle(tmp_path, archive):
     assert text[-1] == "------------ FINISHED EXECUTION ------------"
     assert sum(1 for t in text if t.startswith(" State vector:")) == nroots * k
     assert sum(1 for t in text if t.startswith(" Percent State (1,2):")) == nroots
+
+
+@pytest.mark.parametrize("sys_id", [1, 3])
+def test_spin_orbit_matches_oracle(tmp_path, sys_id):
+    """Spin-orbit parameters of the lowest soroots roots and sodata.in (identify_roots,
+    Source/top.f90:1153-1175, 1231-1252) against the oracle's Ritz vectors and its own
+    formatting, inside the rounding horizon (40 iterations)."""
+    niter, soroots, nroots = 40, 4, 6
+    if sys_id == 1:
+        cfg, h, S = _setup(1, archive_max=200)
+    else:
+        cfg = synth.random_small(91, 3, [4, 4, 3], 2, offdiag_even=False)
+        om, cc, pot = synth.draw_small(cfg)
+        p = L.default_params()
+        p.nstates, p.nmodes, p.ordr, p.niter = 3, 3, 2, niter
+        for i, b in enumerate(cfg.basis):
+            p.basis[i] = b
+        h = L.Handle.from_arrays(p, om, cc, synth.flatten_pot(pot))
+        S = O.system_from_arrays(cfg.basis, 3, 2, om, cc, pot)
+    with h:
+        h.seed()
+        h.lanczos(niter)
+        res = h.spin_orbit(soroots, nroots, str(tmp_path / "sodata.in"))
+    a, b, V, _ = S.lanczos(niter, keep_vectors=True)
+    E, bji, inten, sign, T = O.ritz(a, b)
+    psi = [T[:, r] @ V for r in range(soroots)]
+    fac = inten[:nroots].max()
+    np.testing.assert_allclose(res["energy_ev"], E[:soroots] * O.AU2EV, rtol=1e-12)
+    np.testing.assert_allclose(res["amp"], np.sqrt(inten[:soroots] / fac) * sign[:soroots], rtol=1e-8, atol=1e-12)
+    ns = cfg.nstates
+    for i in range(1, soroots):
+        for j in range(i):
+            bi, bj = psi[i].reshape(ns, -1), psi[j].reshape(ns, -1)
+            ref = bi @ bj.T
+            np.testing.assert_allclose(res["overlap"][i, j], ref, rtol=1e-7, atol=1e-10)
+    assert not res["overlap"][np.triu_indices(soroots)].any()
+    text = (tmp_path / "sodata.in").read_text().splitlines()
+    want = O.sodata_lines(E, inten, sign, psi, soroots, nroots, ns)
+    assert len(text) == len(want)
+    # the root lines are exact; overlap lines agree to the printed digits where the values are
+    # not at the rounding noise of a cancellation
+    assert text[: 2 + soroots + (ns - 1)] == want[: 2 + soroots + (ns - 1)]
+    for t, w in zip(text[2 + soroots + (ns - 1):], want[2 + soroots + (ns - 1):]):
+        assert t[:13] == w[:13]
+        np.testing.assert_allclose([float(x) for x in t[13:].split()], [float(x) for x in w[13:].split()],
+                                   rtol=1e-5, atol=1e-9)
