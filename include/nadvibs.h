@@ -202,6 +202,15 @@ int nvb_lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *sta
 int nvb_spin_orbit(nvb_handle *h, int64_t soroots, int64_t nroots, double *energy_ev, double *amp, double *overlap,
                    const char *sodata_path);
 
+/* Broadening of a line spectrum on the GPU (the post-step programs of the reference):
+ * out[g] = sum_j height[j] f(grid[g] - center[j]) over host arrays, lines summed in order in
+ * FP64, on the current CUDA device.  shape 0: Gaussian of full width at half maximum `width`
+ * (convolve/main.f90:24-43 with convolve/sub.f90's gaussian); shape 1: exp(-t^2/2), t =
+ * (x-c)/width (convolve.py's Gaussian); shape 2: 1/width/(1+t^2) (convolve.py's Lorentzian).
+ * No normalisation (convolve.py divides by the maximum afterwards). */
+int nvb_convolve(const double *center, const double *height, int64_t n, const double *grid, int64_t ngrid,
+                 double width, int64_t shape, double *out);
+
 /* Adjoint contraction of the gradient path (no counterpart in the reference):
  * grad[npot + nstblks + nmodes] = d<u|H(theta)|v>/d theta for theta = (the potterms of
  * nvb_create's layout -- every nadvibs.in expansion coefficient, zero ones included --, the

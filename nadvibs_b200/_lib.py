@@ -53,6 +53,7 @@ _SIGS = {
     "nvb_get_sizes": [C.c_void_p] + [C.c_void_p] * 6,
     "nvb_hv_kernel_in_use": [C.c_void_p, C.c_int64, C.c_void_p],
     "nvb_set_checkpoints": [C.c_void_p, C.c_int64],
+    "nvb_convolve": [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_int64, C.c_void_p],
     "nvb_spin_orbit": [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p],
     "nvb_lanczos_backward": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p],
     "nvb_get_terms": [C.c_void_p] + [C.c_void_p] * 7,
@@ -112,6 +113,21 @@ def dot_noalloc(a_ptr: int, b_ptr: int, n: int, dtype: int, result_ptr: int, str
     """nvb_dot_noalloc: <sa*a, sb*b> written to the device double at result_ptr (no allocation)."""
     check(lib().nvb_dot_noalloc(C.c_void_p(a_ptr), sa, C.c_void_p(b_ptr), sb, n, dtype, C.c_void_p(result_ptr),
                                 C.c_void_p(stream_ptr) if stream_ptr else None))
+
+
+SHAPE_FWHM_GAUSSIAN, SHAPE_GAUSSIAN, SHAPE_LORENTZIAN = 0, 1, 2
+
+
+def convolve(center, height, grid, width: float, shape: int = SHAPE_FWHM_GAUSSIAN) -> np.ndarray:
+    """nvb_convolve: broadened line spectrum on grid (GPU, FP64)."""
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    h = np.ascontiguousarray(height, dtype=np.float64)
+    g = np.ascontiguousarray(grid, dtype=np.float64)
+    if c.shape != h.shape:
+        raise ValueError("center and height differ in length")
+    out = np.zeros(g.size)
+    check(lib().nvb_convolve(_p(c), _p(h), c.size, _p(g), g.size, float(width), int(shape), _p(out)))
+    return out
 
 
 def default_params() -> Params:

@@ -426,6 +426,14 @@ int nvb_hv_adjoint_coeffs(nvb_handle *h, const void *u, const void *v, int64_t d
     });
 }
 
+int nvb_convolve(const double *center, const double *height, int64_t n, const double *grid, int64_t ngrid,
+                 double width, int64_t shape, double *out) {
+    return guarded([&] {
+        if ((n > 0 && (!center || !height)) || (ngrid > 0 && (!grid || !out))) fail(NVB_ERR_ARG, "null argument");
+        convolve_lines(center, height, n, grid, ngrid, width, shape, out);
+    });
+}
+
 int nvb_spin_orbit(nvb_handle *h, int64_t soroots, int64_t nroots, double *energy_ev, double *amp, double *overlap,
                    const char *sodata_path) {
     return guarded([&] {

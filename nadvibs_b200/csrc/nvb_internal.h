@@ -65,6 +65,10 @@ void build_system(System &sys, const nvb_params &p, const double *omega, const d
                   const double *pot);
 int64_t npot_of(const nvb_params &p);
 
+// Spectrum post-step (spectrum.cu)
+void convolve_lines(const double *c, const double *h, int64_t n, const double *grid, int64_t ng, double width,
+                    int64_t shape, double *out);
+
 // Tridiagonal eigensolver (tridiag.cpp)
 void tridiag_eigen(int64_t n, const double *diag, const double *codiag, double *eig, double *vect);
 
