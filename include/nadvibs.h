@@ -227,6 +227,19 @@ int nvb_hv_adjoint_coeffs(nvb_handle *h, const void *u, const void *v, int64_t d
  * Exact derivatives for converged roots. */
 int nvb_hellmann_feynman(nvb_handle *h, int64_t nroots, double *grad, double *energies);
 
+/* Displaced / Duschinsky Franck-Condon seed (shiftref != 0; generate_initialvec's neworigin
+ * branch, Source/secondary.f90:372-726): the seed's state blocks hold <m|n>, the overlap of the
+ * initial vibrational state |m> -- frequencies bomega[nmodes] (hartree) in the coordinates
+ * y = T x + dvec of the Hamiltonian's modes x, T[k][i] = tmat[i*nmodes + k] (column-major, as
+ * nadvibs.in lists it), excited in the first mode with initstate > 0 -- with every product
+ * function |n>.  nvb_create_from_files reads the three blocks from nadvibs.in when basis.in
+ * sets shiftref != 0 (Source/top.f90:130-134); nvb_set_displaced_seed supplies them for a
+ * handle made with nvb_create (before nvb_seed).  nvb_seed_overlap returns
+ * sqrt(sum_n <m|n>^2), the part of the initial state inside the basis (the reference prints
+ * it as "Overlap with the initial state"; 1 for the simple seed). */
+int nvb_set_displaced_seed(nvb_handle *h, const double *bomega, const double *dvec, const double *tmat);
+int nvb_seed_overlap(nvb_handle *h, double *overlap);
+
 /* Record checkpoints of the forward for nvb_lanczos_backward: from the next nvb_seed on,
  * nvb_lanczos saves (v_{c-1}, v_c) at iterations c = 1, 1+k, 1+2k, ... in device memory
  * (2 ceil(niter/k) vectors of the handle's precision).  k = 0 stops recording and frees them.

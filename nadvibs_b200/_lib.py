@@ -53,6 +53,8 @@ _SIGS = {
     "nvb_get_sizes": [C.c_void_p] + [C.c_void_p] * 6,
     "nvb_hv_kernel_in_use": [C.c_void_p, C.c_int64, C.c_void_p],
     "nvb_set_checkpoints": [C.c_void_p, C.c_int64],
+    "nvb_set_displaced_seed": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "nvb_seed_overlap": [C.c_void_p, C.c_void_p],
     "nvb_convolve": [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_int64, C.c_void_p],
     "nvb_spin_orbit": [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p],
     "nvb_lanczos_backward": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p],
@@ -322,6 +324,19 @@ class Handle:
         check(lib().nvb_spin_orbit(self.ptr, soroots, nroots, _p(e), _p(amp), _p(ov),
                                    None if path is None else path.encode()))
         return dict(energy_ev=e, amp=amp, overlap=ov)
+
+    def set_displaced_seed(self, bomega, dvec, tmat):
+        """nvb_set_displaced_seed: initial-state frequencies, displacement, Duschinsky matrix
+        (column-major flat, tmat[i*nmodes + k] = T[k, i])."""
+        b = np.ascontiguousarray(bomega, dtype=np.float64)
+        d = np.ascontiguousarray(dvec, dtype=np.float64)
+        t = np.ascontiguousarray(tmat, dtype=np.float64).reshape(-1)
+        check(lib().nvb_set_displaced_seed(self.ptr, _p(b), _p(d), _p(t)))
+
+    def seed_overlap(self) -> float:
+        v = C.c_double()
+        check(lib().nvb_seed_overlap(self.ptr, C.byref(v)))
+        return v.value
 
     def set_checkpoints(self, k: int):
         """Record (v_{c-1}, v_c) every k iterations from the next seed (nvb_set_checkpoints)."""

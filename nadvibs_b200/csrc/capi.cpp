@@ -156,11 +156,14 @@ int nvb_create_from_files(const char *basis_path, const char *nadvibs_path, cons
         nvb_params p;
         nvb_params_default(&p);
         parse_basis_text(read_file(basis_path), p);
-        if (p.shiftref != 0) fail(NVB_ERR_ARG, "shiftref != 0 (Duschinsky seed) is not supported");
-        std::vector<double> om, cc, pot;
-        parse_nadvibs_text(read_file(nadvibs_path), p, om, cc, pot);
+        std::vector<double> om, cc, pot, disp;
+        parse_nadvibs_text(read_file(nadvibs_path), p, om, cc, pot, &disp);
         h = new nvb_handle();
         create_common(h, p, om.data(), cc.data(), pot.data(), opt);
+        if (p.shiftref != 0) {
+            const int64_t M = p.nmodes;
+            set_displaced(h->sys, disp.data(), disp.data() + M, disp.data() + 2 * M);
+        }
     });
     if (rc != NVB_OK) {
         if (h) nvb_destroy(h);
@@ -183,6 +186,7 @@ int nvb_destroy(nvb_handle *h) {
             slab_free(h->slab[1]);
             quad_free(h->quad);
             ckpt_free(h);
+            if (h->seed_vec) cudaFree(h->seed_vec);
             if (h->own_stream) cudaStreamDestroy(h->own_stream);
         }
     });
@@ -440,6 +444,29 @@ int nvb_spin_orbit(nvb_handle *h, int64_t soroots, int64_t nroots, double *energ
         if (!h) fail(NVB_ERR_ARG, "null handle");
         ensure_device(h);
         spin_orbit(h, soroots, nroots, energy_ev, amp, overlap, sodata_path);
+    });
+}
+
+int nvb_set_displaced_seed(nvb_handle *h, const double *bomega, const double *dvec, const double *tmat) {
+    return guarded([&] {
+        if (!h || !bomega || !dvec || !tmat) fail(NVB_ERR_ARG, "null argument");
+        set_displaced(h->sys, bomega, dvec, tmat);
+        if (h->seed_vec) cudaFree(h->seed_vec);
+        h->seed_vec = nullptr;
+        h->seed_norm = 0.0;
+    });
+}
+
+int nvb_seed_overlap(nvb_handle *h, double *overlap) {
+    return guarded([&] {
+        if (!h || !overlap) fail(NVB_ERR_ARG, "null argument");
+        if (!h->sys.neworigin) {
+            *overlap = 1.0;
+            return;
+        }
+        ensure_device(h);
+        if (!h->seed_vec) displaced_seed(h);
+        *overlap = h->seed_norm;
     });
 }
 

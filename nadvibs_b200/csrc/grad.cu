@@ -183,32 +183,7 @@ static void replay_segment(nvb_handle *h, void *b3[3], double sprev, double scur
 
 // The seed vector in native precision into buf (as lanczos_seed builds it); returns its scale.
 static double seed_native(nvb_handle *h, void *buf) {
-    const int S = h->sys.S;
-    std::vector<double> w(h->sys.prm.weights, h->sys.prm.weights + S);
-    if ((int)h->seed_w.size() == S) w = h->seed_w;
-    double wsum = 0.0;
-    for (double v : w) wsum += v;
-    if (wsum == 0.0) wsum = 1.0;
-    double d2 = 0.0;
-    std::vector<double> q(S);
-    for (int s = 0; s < S; ++s) {
-        q[s] = 1.0 * (w[s] / (wsum * 1.0));
-        d2 += std::fabs(q[s]) * std::fabs(q[s]);
-    }
-    const double scl = 1.0 / std::sqrt(d2);
-    CK(cudaMemsetAsync(buf, 0, (size_t)h->ntotal() * h->elem_size(), h->stream));
-    for (int s = 0; s < S; ++s) {
-        const double v = q[s] * scl;
-        if (h->precision == NVB_MIXED) {
-            const float fv = (float)v;
-            CK(cudaMemcpyAsync((float *)buf + (size_t)s * h->sys.dimen, &fv, sizeof(float), cudaMemcpyHostToDevice,
-                               h->stream));
-        } else {
-            CK(cudaMemcpyAsync((double *)buf + (size_t)s * h->sys.dimen, &v, sizeof(double), cudaMemcpyHostToDevice,
-                               h->stream));
-        }
-        CK(cudaStreamSynchronize(h->stream));
-    }
+    seed_fill(h, buf, seed_weights(h));
     return 1.0 / h->beta[0];
 }
 

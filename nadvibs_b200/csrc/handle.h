@@ -52,6 +52,9 @@ struct nvb_handle {
     int64_t ck_k = 0, ck_count = 0, ck_cap = 0;
     void *ck_buf = nullptr;
     double *ck_scale = nullptr;
+    // displaced / Duschinsky seed: <m|n> over one state block (FP64) and its norm
+    double *seed_vec = nullptr;
+    double seed_norm = 0.0;
     // cached scratch for ad-hoc vectors
     void *tmp = nullptr;
     size_t tmp_bytes = 0;
@@ -79,6 +82,9 @@ void save_restart(nvb_handle *h, const char *dir, const char *vdir);
 void load_restart(nvb_handle *h, const char *dir, const char *vdir);
 void hv_adjoint(nvb_handle *h, const void *u, const void *v, int dtype, double *grad);
 void hellmann_feynman(nvb_handle *h, int64_t nroots, double *grad, double *energies);
+void displaced_seed(nvb_handle *h);
+double seed_fill(nvb_handle *h, void *buf, const std::vector<double> &w);
+std::vector<double> seed_weights(const nvb_handle *h);
 void ckpt_reserve(nvb_handle *h, int64_t total_iters);
 void ckpt_save(nvb_handle *h, int64_t it);
 void ckpt_free(nvb_handle *h);

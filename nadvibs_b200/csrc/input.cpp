@@ -242,7 +242,7 @@ struct ListReader {
 }  // namespace
 
 void parse_nadvibs_text(const std::string &text, const nvb_params &p, std::vector<double> &omega,
-                        std::vector<double> &concoef, std::vector<double> &pot) {
+                        std::vector<double> &concoef, std::vector<double> &pot, std::vector<double> *displaced) {
     ListReader rd(text);
     const int64_t nstblks = p.nstates * (p.nstates + 1) / 2;
     omega.clear(); concoef.clear(); pot.clear();
@@ -256,6 +256,29 @@ void parse_nadvibs_text(const std::string &text, const nvb_params &p, std::vecto
             rd.values(numut(p.nmodes, d), pot, "expansion coefficients");
         }
     }
+    // the initial state's frequencies, displacement and Duschinsky matrix (Source/top.f90:130-134)
+    if (displaced && p.shiftref != 0) {
+        displaced->clear();
+        rd.skip("initial-state frequencies");
+        rd.values(p.nmodes, *displaced, "initial-state frequencies");
+        rd.skip("displacement");
+        rd.values(p.nmodes, *displaced, "displacement");
+        rd.skip("Duschinsky matrix");
+        rd.values(p.nmodes * p.nmodes, *displaced, "Duschinsky matrix");
+    }
+}
+
+void set_displaced(System &sys, const double *bomega, const double *dvec, const double *tmat) {
+    const int M = sys.M;
+    for (int i = 0; i < M; ++i)
+        if (!(bomega[i] > 0.0) || !std::isfinite(bomega[i]) || !std::isfinite(dvec[i]))
+            fail(NVB_ERR_ARG, "initial-state frequencies must be positive and displacements finite");
+    for (int i = 0; i < M * M; ++i)
+        if (!std::isfinite(tmat[i])) fail(NVB_ERR_ARG, "non-finite Duschinsky matrix");
+    sys.bomega.assign(bomega, bomega + M);
+    sys.dvec.assign(dvec, dvec + M);
+    sys.tmat.assign(tmat, tmat + (size_t)M * M);
+    sys.neworigin = true;
 }
 
 // ------------------------------------------------------------------ term compiler
@@ -264,7 +287,6 @@ void build_system(System &sys, const nvb_params &p, const double *omega, const d
     if (p.nstates < 1 || p.nstates > MAX_STATES) fail(NVB_ERR_ARG, "nstates must be in 1..10");
     if (p.nmodes < 1 || p.nmodes > MAX_MODES) fail(NVB_ERR_ARG, "nmodes must be in 1..64");
     if (p.ordr < 1 || p.ordr > MAX_ORDER) fail(NVB_ERR_ARG, "ordr must be in 1..4 (<m|x^p|n> is tabulated to p=4)");
-    if (p.shiftref != 0) fail(NVB_ERR_ARG, "shiftref != 0 (Duschinsky seed) is not supported");
     sys.prm = p;
     sys.S = (int)p.nstates;
     sys.M = (int)p.nmodes;
@@ -280,6 +302,21 @@ void build_system(System &sys, const nvb_params &p, const double *omega, const d
     sys.shft.assign(sys.M, 1);
     for (int k = 0; k < sys.M; ++k)
         for (int j = k + 1; j < sys.M; ++j) sys.shft[k] *= sys.nfunc[j];
+    // symmetry blocks of the modes (npirr, Source/secondary.f90:396-405) and the initial state:
+    // only its first excited mode counts (Source/top.f90:326-334)
+    sys.irrep.assign(sys.M, 0);
+    {
+        int m = 0;
+        for (int l = 0; l < 10 && m < sys.M; ++l)
+            for (int64_t c = 0; c < p.npirr[l] && m < sys.M; ++c) sys.irrep[m++] = l;
+    }
+    sys.istate.assign(sys.M, 0);
+    for (int i = 0; i < sys.M; ++i)
+        if (p.initstate[i] > 0) {
+            if (p.initstate[i] > 100) fail(NVB_ERR_ARG, "initstate above 100 quanta");
+            sys.istate[i] = p.initstate[i];
+            break;
+        }
     sys.omega.assign(omega, omega + sys.M);
     for (double w : sys.omega)
         if (!(w > 0.0) || !std::isfinite(w)) fail(NVB_ERR_ARG, "frequencies must be positive and finite");

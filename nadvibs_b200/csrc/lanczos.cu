@@ -238,23 +238,37 @@ void lanczos_free(nvb_handle *h) {
     h->tmp_bytes = 0;
 }
 
-// generate_initialvec, simple branch (Source/secondary.f90:727-783): q3 = 0 except row 1 of
-// every state = 1; d1 = sqrt(<q3,q3>/nstates) = 1; state i scaled by statew(i)/(sum(statew)*d1);
-// the vector normalised; beta(0) = ||q3||.
-void lanczos_seed(nvb_handle *h, const double *weights) {
+template <typename T>
+__global__ void k_seed_vec(T *__restrict__ v, const double *__restrict__ o, long long dimen, int S,
+                           const double *__restrict__ q, double inv) {
+    const long long n = dimen * S;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const long long s = i / dimen, r = i - s * dimen;
+        v[i] = (T)(q[s] * (o[r] * inv));
+    }
+}
+
+std::vector<double> seed_weights(const nvb_handle *h) {
     const int S = h->sys.S;
-    if (!h->buf[0]) lanczos_alloc(h);
-    std::vector<double> w(S);
-    for (int s = 0; s < S; ++s) w[s] = weights ? weights[s] : h->sys.prm.weights[s];
-    h->seed_w = w;
+    if ((int)h->seed_w.size() == S) return h->seed_w;
+    return std::vector<double>(h->sys.prm.weights, h->sys.prm.weights + S);
+}
+
+// The seed of generate_initialvec (Source/secondary.f90:351-783) in the handle's precision
+// into buf; returns beta(0), the norm of the stored vector.  Simple branch: q3 = 0 except row 1
+// of every state = 1, so d1 = sqrt(<q3,q3>/nstates) = 1.  Displaced branch (shiftref != 0):
+// every state block holds <m|n> (seed.cu), d1 = sqrt(sum_n <m|n>^2).  Then state i is scaled
+// by statew(i)/(sum(statew)*d1) and the vector normalised.
+double seed_fill(nvb_handle *h, void *buf, const std::vector<double> &w) {
+    const int S = h->sys.S;
     double wsum = 0.0;
     for (double v : w) wsum += v;
     if (wsum == 0.0) wsum = 1.0;
-    const double d1 = 1.0;
     std::vector<double> q(S);
     double d2 = 0.0;
     for (int s = 0; s < S; ++s) {
-        q[s] = 1.0 * (w[s] / (wsum * d1));
+        q[s] = 1.0 * (w[s] / (wsum * 1.0));
         const double e = std::sqrt(q[s] * q[s]);
         d2 += e * e;
     }
@@ -265,22 +279,49 @@ void lanczos_seed(nvb_handle *h, const double *weights) {
         q[s] *= scl;
         nrm += q[s] * q[s];
     }
-    if (h->precision == NVB_MIXED) {
+    const bool mixed = h->precision == NVB_MIXED;
+    if (mixed) {
         nrm = 0.0;
         for (int s = 0; s < S; ++s) nrm += (double)(float)q[s] * (double)(float)q[s];
     }
-    const double beta0 = std::sqrt(nrm);
     double *dw = nullptr;
     CK(cudaMalloc((void **)&dw, S * sizeof(double)));
     CK(cudaMemcpyAsync(dw, q.data(), S * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    const long long n = h->ntotal();
+    double beta0 = std::sqrt(nrm);
+    if (!h->sys.neworigin) {
+        if (mixed) k_seed<float><<<grid_for(n), RED_THREADS, 0, h->stream>>>((float *)buf, h->sys.dimen, S, dw);
+        else k_seed<double><<<grid_for(n), RED_THREADS, 0, h->stream>>>((double *)buf, h->sys.dimen, S, dw);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(h->stream));
+    } else {
+        if (!h->seed_vec) displaced_seed(h);
+        if (!(h->seed_norm > 0.0)) fail(NVB_ERR_ARG, "displaced seed: the initial state has no overlap with the basis");
+        const double inv = 1.0 / h->seed_norm;
+        if (mixed)
+            k_seed_vec<float><<<grid_for(n), RED_THREADS, 0, h->stream>>>((float *)buf, h->seed_vec, h->sys.dimen, S,
+                                                                         dw, inv);
+        else
+            k_seed_vec<double><<<grid_for(n), RED_THREADS, 0, h->stream>>>((double *)buf, h->seed_vec, h->sys.dimen,
+                                                                          S, dw, inv);
+        CK(cudaGetLastError());
+        beta0 = std::sqrt(device_dot(h, buf, 1.0, buf, 1.0, mixed ? NVB_DTYPE_F32 : NVB_DTYPE_F64));
+    }
+    cudaFree(dw);
+    return beta0;
+}
+
+// generate_initialvec (Source/secondary.f90:351-783): the seed (seed_fill), v(0) = 0,
+// beta(0) = ||seed||.
+void lanczos_seed(nvb_handle *h, const double *weights) {
+    const int S = h->sys.S;
+    if (!h->buf[0]) lanczos_alloc(h);
+    std::vector<double> w(S);
+    for (int s = 0; s < S; ++s) w[s] = weights ? weights[s] : h->sys.prm.weights[s];
+    h->seed_w = w;
     h->cur = 0; h->prev = 1; h->work = 2;
     const long long n = h->ntotal();
-    if (h->precision == NVB_MIXED) {
-        k_seed<float><<<grid_for(n), RED_THREADS, 0, h->stream>>>((float *)h->buf[h->cur], h->sys.dimen, S, dw);
-    } else {
-        k_seed<double><<<grid_for(n), RED_THREADS, 0, h->stream>>>((double *)h->buf[h->cur], h->sys.dimen, S, dw);
-    }
-    CK(cudaGetLastError());
+    const double beta0 = seed_fill(h, h->buf[h->cur], w);
     CK(cudaMemsetAsync(h->buf[h->prev], 0, (size_t)n * h->elem_size(), h->stream));
     double sc[3] = {0, 0, 0};
     sc[h->cur] = 1.0 / beta0;
@@ -289,7 +330,6 @@ void lanczos_seed(nvb_handle *h, const double *weights) {
     CK(cudaMemsetAsync(h->d_beta, 0, sizeof(double), h->stream));
     CK(cudaMemcpyAsync(h->d_beta, &beta0, sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    cudaFree(dw);
     h->alpha.assign(1, 0.0);
     h->beta.assign(1, beta0);
     h->iters = 0;

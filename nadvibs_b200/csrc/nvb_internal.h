@@ -51,13 +51,20 @@ struct System {
     std::vector<double> potterms;     // file layout [block][order][monomial]
     std::vector<int64_t> pot_offset;  // [nstblks*ordr] start of each (block, order)
     std::vector<Term> terms;
+    // displaced / Duschinsky seed (shiftref != 0, Source/secondary.f90:372-726)
+    bool neworigin = false;
+    std::vector<double> bomega, dvec, tmat;  // initial-state frequencies, displacement, T (column-major)
+    std::vector<int> irrep;                  // symmetry block of every mode (npirr)
+    std::vector<int64_t> istate;             // initial-state quanta, at most one mode excited
     int nstblks() const { return S * (S + 1) / 2; }
 };
 
 // Parsing / term compilation (input.cpp)
 void parse_basis_text(const std::string &text, nvb_params &p);
 void parse_nadvibs_text(const std::string &text, const nvb_params &p, std::vector<double> &omega,
-                        std::vector<double> &concoef, std::vector<double> &pot);
+                        std::vector<double> &concoef, std::vector<double> &pot,
+                        std::vector<double> *displaced = nullptr);  // bomega | dvec | tmat when shiftref != 0
+void set_displaced(System &sys, const double *bomega, const double *dvec, const double *tmat);
 std::string read_file(const std::string &path);
 int64_t numut(int64_t n, int64_t d);
 std::vector<std::vector<int>> monomials(int nmodes, int order);  // file order, 1-based digits

@@ -427,34 +427,9 @@ static void ritz_vectors(nvb_handle *h, int64_t nroots, const std::vector<double
         const size_t per = (size_t)N * h->elem_size();
         void *b3[3] = {nullptr, nullptr, nullptr};
         for (int i = 0; i < 3; ++i) CK(cudaMalloc(&b3[i], per));
-        // seed: the same vector lanczos_seed builds
-        // the seed's weights: those nvb_seed used, or basis.in's after a restart
-        std::vector<double> w(h->sys.prm.weights, h->sys.prm.weights + h->sys.S);
-        if ((int)h->seed_w.size() == h->sys.S) w = h->seed_w;
-        double wsum = 0.0;
-        for (double v : w) wsum += v;
-        if (wsum == 0.0) wsum = 1.0;
-        double d2 = 0.0;
-        std::vector<double> q(h->sys.S);
-        for (int s = 0; s < h->sys.S; ++s) {
-            q[s] = 1.0 * (w[s] / (wsum * 1.0));
-            d2 += std::fabs(q[s]) * std::fabs(q[s]);
-        }
-        const double scl = 1.0 / std::sqrt(d2);
-        CK(cudaMemsetAsync(b3[0], 0, per, h->stream));
+        // the seed lanczos_seed built (the weights nvb_seed used, or basis.in's after a restart)
+        seed_fill(h, b3[0], seed_weights(h));
         CK(cudaMemsetAsync(b3[1], 0, per, h->stream));
-        for (int s = 0; s < h->sys.S; ++s) {
-            const double v = q[s] * scl;
-            if (mixed) {
-                const float fv = (float)v;
-                CK(cudaMemcpyAsync((float *)b3[0] + (size_t)s * h->sys.dimen, &fv, sizeof(float), cudaMemcpyHostToDevice,
-                                   h->stream));
-            } else {
-                CK(cudaMemcpyAsync((double *)b3[0] + (size_t)s * h->sys.dimen, &v, sizeof(double), cudaMemcpyHostToDevice,
-                                   h->stream));
-            }
-            CK(cudaStreamSynchronize(h->stream));
-        }
         int cur = 0, prev = 1, work = 2;
         double scur = 1.0 / h->beta[0], sprev = 0.0;
         const int dt = mixed ? NVB_DTYPE_F32 : NVB_DTYPE_F64;

@@ -164,8 +164,10 @@ def _fmt_vals(vals, per_line=4) -> str:
     return "\n".join(lines) + "\n"
 
 
-def write_nadvibs_in(path: str, nmodes: int, omega, concoef, pot) -> None:
-    """Write ``nadvibs.in`` in the layout read by Source/top.f90:122-135 (no new origin)."""
+def write_nadvibs_in(path: str, nmodes: int, omega, concoef, pot, displaced=None) -> None:
+    """Write ``nadvibs.in`` in the layout read by Source/top.f90:122-135; ``displaced`` =
+    (bomega, dvec, tmat) appends the initial-state blocks read when shiftref != 0
+    (Source/top.f90:130-134; tmat column-major, tmat[i*nmodes + k] = T[k, i])."""
     S_blocks = len(concoef)
     with open(path, "w") as f:
         f.write(" FREQUENCIES (hartree)\n")
@@ -176,9 +178,17 @@ def write_nadvibs_in(path: str, nmodes: int, omega, concoef, pot) -> None:
             for d, vals in enumerate(pot[b], start=1):
                 f.write(f" BLOCK {b + 1} ORDER {d}\n")
                 f.write(_fmt_vals(vals))
+        if displaced is not None:
+            bomega, dvec, tmat = displaced
+            f.write(" INITIAL-STATE FREQUENCIES (hartree)\n")
+            f.write(_fmt_vals(bomega))
+            f.write(" DISPLACEMENT\n")
+            f.write(_fmt_vals(dvec))
+            f.write(" DUSCHINSKY MATRIX (column-major)\n")
+            f.write(_fmt_vals(tmat))
 
 
-def write_basis_in(path: str, cfg: SynthConfig, niter: int | None = None, **over) -> None:
+def write_basis_in(path: str, cfg: SynthConfig, niter: int | None = None, initstate=None, **over) -> None:
     """Write the ``&NADVIBS`` namelist (keys of Source/secondary.f90:844-845)."""
     kv = dict(niter=cfg.niter if niter is None else niter, natoms=max(2, (cfg.nmodes + 6) // 3),
               nmodes=cfg.nmodes, nstates=cfg.nstates, ordr=cfg.ordr, restart=0,
@@ -192,7 +202,8 @@ def write_basis_in(path: str, cfg: SynthConfig, niter: int | None = None, **over
             f.write(f"  {k} = {v},\n")
         f.write("  basis = " + ", ".join(str(b) for b in cfg.basis) + ",\n")
         f.write("  npirr = " + str(cfg.nmodes) + ",\n")
-        f.write("  initstate = " + ", ".join("0" for _ in cfg.basis) + ",\n")
+        ist = [0] * cfg.nmodes if initstate is None else list(initstate)
+        f.write("  initstate = " + ", ".join(str(int(v)) for v in ist) + ",\n")
         f.write("  weights = " + ", ".join(f"{w:.6f}" for w in weights) + "\n")
         f.write(" /\n")
 
