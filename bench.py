@@ -37,7 +37,7 @@ CONFIG_NUMBER = 2
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both")
@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--config", type=int, default=CONFIG_NUMBER)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient (grad/fwd) measurement")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the mixed-vs-FP64 Ritz comparison")
     ap.add_argument("--basis", type=str, default=None,
                     help="comma-separated basis overriding the config's (same coefficients; profiling of "
                          "reduced sizes)")
@@ -207,6 +208,38 @@ def run_ours(args, rank, world, dev):
     return cfg, N, results, e2e
 
 
+def mixed_accuracy(basis: str, nadvibs: str, dev: int, iters: int = 300):
+    """Mixed precision against FP64 on the benchmark system: both precisions run `iters` plain
+    Lanczos iterations from the same seed; every FP64 Ritz value converged to 1e-8 (bji) with
+    intensity >= 1e-4 is matched to the nearest mixed Ritz value (energy difference in cm^-1)
+    and its intensity compared with the mixed intensity summed over Ritz values within
+    0.5 cm^-1 (ghost copies split a line)."""
+    import numpy as np
+    from nadvibs_b200 import _lib as L
+    au2cm = 219474.6313705
+    out = {}
+    for prec in (L.NVB_FP64, L.NVB_MIXED):
+        h = L.Handle.from_files(basis, nadvibs, device=dev, precision=prec)
+        h.seed()
+        h.lanczos(iters)
+        out[prec] = h.ritz(iters)
+        h.close()
+    E, bji, inten = out[L.NVB_FP64][:3]
+    Em, _, intm = out[L.NVB_MIXED][:3]
+    conv = (bji < 1e-8) & (inten > 1e-4)
+    dE, dI = [], []
+    for e, i in zip(E[conv], inten[conv]):
+        dE.append(abs(Em[np.argmin(np.abs(Em - e))] - e) * au2cm)
+        i64 = inten[np.abs(E - e) * au2cm < 0.5].sum()
+        i32 = intm[np.abs(Em - e) * au2cm < 0.5].sum()
+        if i64 >= 1e-3:
+            dI.append(abs(i32 - i64) / i64)
+    return {"iterations": iters, "converged_roots": int(conv.sum()),
+            "max_abs_dE_cm": float(max(dE)) if dE else None,
+            "max_rel_dI": float(max(dI)) if dI else None,
+            "target_dE_cm": 0.1}
+
+
 def grad_timing(dev: int):
     """grad/fwd on the gradient system (config 4): forward = seed + 400 plain Lanczos
     iterations recording checkpoints every 50; backward = eigen-derivatives of T_400 for a
@@ -333,6 +366,10 @@ def main():
         line["fp64_hv_ms"] = r["hv_ms_per"]
     if rank == 0 and not args.no_grad:
         line["grad"] = grad_timing(local)
+    if rank == 0 and "mixed" in res and not args.no_accuracy:
+        tmp = tempfile.mkdtemp(prefix="nvb_acc_")
+        _, (b_in, n_in) = make_inputs(args.config, tmp, args.basis)
+        line["accuracy"] = mixed_accuracy(b_in, n_in, local)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(args.config, 1)
     if rank == 0:
