@@ -124,7 +124,16 @@ int nvb_set_precision(nvb_handle *h, int64_t precision);
  * cudaStreamLegacy for the legacy default stream); NULL restores the handle-owned stream,
  * which does not synchronise with the legacy default stream. */
 int nvb_set_stream(nvb_handle *h, void *stream);
+/* Waits for the handle's stream and reports a tiled H.v kernel that gave up waiting for a
+ * shared-memory copy (NVB_ERR_CUDA; the error is reported once and the handle stays usable). */
 int nvb_synchronize(nvb_handle *h);
+
+/* Failure-detection test hook (no reference counterpart): mode 1 makes the factorised
+ * quadratic H.v kernel issue none of its copies, so every wait of its consumer warps runs out
+ * (after a short poll limit in this mode); the kernel raises its abort flag, finishes without
+ * touching the missing data and sets its error word, which the next nvb_synchronize /
+ * nvb_lanczos reports as NVB_ERR_CUDA.  Mode 0 (default) restores normal operation. */
+int nvb_set_fault_test(nvb_handle *h, int64_t mode);
 
 /* y = H x on device pointers of dtype NVB_DTYPE_F64 or NVB_DTYPE_F32 (both vectors the same
  * dtype).  Replaces Hv (Source/top.f90:672-818).  Stream-ordered, asynchronous. */

@@ -53,6 +53,7 @@ _SIGS = {
     "nvb_get_sizes": [C.c_void_p] + [C.c_void_p] * 6,
     "nvb_hv_kernel_in_use": [C.c_void_p, C.c_int64, C.c_void_p],
     "nvb_set_checkpoints": [C.c_void_p, C.c_int64],
+    "nvb_set_fault_test": [C.c_void_p, C.c_int64],
     "nvb_set_displaced_seed": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_seed_overlap": [C.c_void_p, C.c_void_p],
     "nvb_convolve": [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_int64, C.c_void_p],
@@ -337,6 +338,10 @@ class Handle:
         v = C.c_double()
         check(lib().nvb_seed_overlap(self.ptr, C.byref(v)))
         return v.value
+
+    def set_fault_test(self, mode: int):
+        """nvb_set_fault_test: 1 = the quadratic H.v kernel issues no copies (its waits run out)."""
+        check(lib().nvb_set_fault_test(self.ptr, mode))
 
     def set_checkpoints(self, k: int):
         """Record (v_{c-1}, v_c) every k iterations from the next seed (nvb_set_checkpoints)."""

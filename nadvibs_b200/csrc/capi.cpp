@@ -272,6 +272,15 @@ int nvb_synchronize(nvb_handle *h) {
         if (!h) fail(NVB_ERR_ARG, "null handle");
         ensure_device(h);
         CKA(cudaStreamSynchronize(h->stream));
+        check_kernel_flags(h);
+    });
+}
+
+int nvb_set_fault_test(nvb_handle *h, int64_t mode) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        if (mode != 0 && mode != 1) fail(NVB_ERR_ARG, "fault-test mode must be 0 or 1");
+        h->quad.test_nocopy = (int)mode;
     });
 }
 

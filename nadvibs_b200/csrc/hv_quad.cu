@@ -36,6 +36,8 @@ struct QuadArgs {
     const int *item_beg;
     int *err;
     int M, m, nmax, nv, pad, sstate, TF, ntiles, nslot, nitems;
+    int nocopy;      // failure test: the producer issues no copy, so every consumer wait runs out
+    int wait_limit;  // polls before a wait gives up
     long long dimen;
     unsigned dpm;
     QuadFast<T> F;
@@ -72,10 +74,11 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, unsigned parity) {
     return ok != 0;
 }
 
-// Bounded wait on a phase; gives up (and raises the abort flag) after WAIT_LIMIT polls, or
-// early once another thread raised it.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, volatile int *abort_flag) {
-    for (int i = 0; i < WAIT_LIMIT; ++i) {
+// Bounded wait on a phase; gives up (and raises the abort flag) after `limit` polls, or early
+// once another thread raised it.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, volatile int *abort_flag,
+                                          int limit = WAIT_LIMIT) {
+    for (int i = 0; i < limit; ++i) {
         if (mbar_try(bar, parity)) return true;
         if ((i & 255) == 255 && *abort_flag) return false;
     }
@@ -178,7 +181,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
         int slot = 0;
         unsigned ph = 0;
         long long issued = 0;
-        int stop = 0;
+        int stop = A.nocopy;
         for (int tile = blockIdx.x; tile < A.ntiles && !stop; tile += gridDim.x) {
             unsigned myw = 0;
             for (int w = 0; w < nw; ++w) {
@@ -207,7 +210,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                     bits &= bits - 1;
                     if (lane == 0 && !stop) {
                         const QuadItem q = s_it[it];
-                        if (mbar_wait(&empty[slot], ph ^ 1u, abort_flag)) {
+                        if (mbar_wait(&empty[slot], ph ^ 1u, abort_flag, A.wait_limit)) {
                             mbar_expect_tx(&full[slot], bytes);
                             bulk_g2s(s_ring + slot * sst + pad, x + q.b * N + tb + (long long)q.tshift * TF, bytes,
                                      &full[slot]);
@@ -348,7 +351,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
             for (int it = s_ib[a]; it < iend; ++it) {
                 const int f = fl[it];
                 if (f == 0) continue;
-                const bool ok = mbar_try(&full[slot], ph) || mbar_wait(&full[slot], ph, abort_flag);
+                const bool ok = mbar_try(&full[slot], ph) || mbar_wait(&full[slot], ph, abort_flag, A.wait_limit);
                 const T *buf = s_ring + slot * sst + pad;
                 if (ok) {
                     if (f <= 2) {
@@ -543,6 +546,8 @@ QuadArgs<T> quad_args(const QuadPlan &qp) {
     a.items = qp.d_items;
     a.item_beg = qp.d_item_beg;
     a.err = qp.d_err;
+    a.nocopy = qp.test_nocopy;
+    a.wait_limit = qp.test_nocopy ? (1 << 14) : WAIT_LIMIT;
     a.M = qp.M;
     a.m = qp.m;
     a.nmax = qp.nmax;

@@ -173,13 +173,19 @@ void check_kernel_flags(nvb_handle *h) {
     if (h->quad.ok && h->quad.d_err) {
         int e = 0;
         CK(cudaMemcpy(&e, h->quad.d_err, sizeof(int), cudaMemcpyDeviceToHost));
-        if (e) fail(NVB_ERR_CUDA, "quadratic H.v: a shared-memory tile copy did not complete (kernel gave up waiting)");
+        if (e) {
+            CK(cudaMemset(h->quad.d_err, 0, sizeof(int)));  // reported once; the handle stays usable
+            fail(NVB_ERR_CUDA, "quadratic H.v: a shared-memory tile copy did not complete (kernel gave up waiting)");
+        }
     }
     for (int i = 0; i < 2; ++i)
         if (h->slab[i].ok && h->slab[i].d_err) {
             int e = 0;
             CK(cudaMemcpy(&e, h->slab[i].d_err, sizeof(int), cudaMemcpyDeviceToHost));
-            if (e) fail(NVB_ERR_CUDA, "slab H.v: a shared-memory tile copy did not complete (kernel gave up waiting)");
+            if (e) {
+                CK(cudaMemset(h->slab[i].d_err, 0, sizeof(int)));
+                fail(NVB_ERR_CUDA, "slab H.v: a shared-memory tile copy did not complete (kernel gave up waiting)");
+            }
         }
 }
 

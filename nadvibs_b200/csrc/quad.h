@@ -87,6 +87,7 @@ struct QuadPlan {
     int *d_err = nullptr;
     size_t smem[2] = {0, 0};  // FP64, FP32
     int grid[2] = {0, 0};
+    int test_nocopy = 0;      // failure test (nvb_set_fault_test): no copies, waits run out
 };
 
 // Shared-memory layout (byte offsets), identical on host and device.
