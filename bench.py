@@ -242,9 +242,9 @@ def mixed_accuracy(basis: str, nadvibs: str, dev: int, iters: int = 300):
 
 def grad_timing(dev: int):
     """grad/fwd on the gradient system (config 4): forward = seed + 400 plain Lanczos
-    iterations recording checkpoints every 50; backward = eigen-derivatives of T_400 for a
-    loss (Gaussian-convolved spectrum, sigma 20 cm^-1, 2048 points, plus the lowest 20 Ritz
-    energies) and the reverse sweep (nvb_lanczos_backward).  Host wall times around
+    iterations; backward = eigen-derivatives of T_400 for a loss (Gaussian-convolved spectrum,
+    sigma 20 cm^-1, 2048 points, plus the lowest 20 Ritz energies) and the reverse sweep
+    (nvb_lanczos_backward with the automatic checkpoint plan, k = 0).  Host wall times around
     synchronised calls, best of 3."""
     import numpy as np
     import torch
@@ -258,13 +258,13 @@ def grad_timing(dev: int):
     p.nstates, p.nmodes, p.ordr, p.niter = cfg.nstates, cfg.nmodes, cfg.ordr, cfg.niter
     for i, b in enumerate(cfg.basis):
         p.basis[i] = b
-    n, k = 400, 50
+    n, k = 400, 0
     grid = torch.linspace(-200.0, 8000.0, 2048, dtype=torch.float64)
     w = torch.from_numpy(np.random.default_rng(4).normal(size=2048))
     fwd, bwd = [], []
+    plan = None
     for _ in range(3):
         h = L.Handle.from_arrays(p, om, cc, potf, device=dev)
-        h.set_checkpoints(k)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         h.seed()
@@ -281,12 +281,14 @@ def grad_timing(dev: int):
         h.lanczos_backward(n, abar, bbar, k)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
+        plan = h.backward_plan()
         h.close()
         fwd.append(t1 - t0)
         bwd.append(t2 - t1)
     f, g = min(fwd), min(bwd)
     return {"workload": "config4: 2 states, basis [14,12,10,8,8,6], 1,290,240 functions, ordr 2, 400 plain "
-                        "Lanczos iterations, checkpoints every 50, FP64",
+                        "Lanczos iterations, automatic checkpoint plan, FP64",
+            "backward_plan": plan,
             "loss": "Gaussian-convolved spectrum (sigma 20 cm^-1, 2048 points) + lowest 20 Ritz energies",
             "ncoef": int(len(potf) + len(cc) + len(om)), "fwd_ms": 1e3 * f, "grad_ms": 1e3 * g,
             "grad_over_fwd": g / f}

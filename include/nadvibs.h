@@ -258,13 +258,34 @@ int nvb_set_checkpoints(nvb_handle *h, int64_t k);
 /* Reverse sweep through the first n Lanczos iterations (plain Lanczos, reorthog = 0): given
  * alpha_bar[i-1] = dL/dalpha_i and beta_bar[i-1] = dL/dbeta_i (i = 1..n; beta_bar may be NULL
  * for zeros) of a loss L of T_n, returns grad[ncoef] = dL/dtheta in the layout of
- * nvb_hv_adjoint_coeffs.  Primal vectors are recomputed segment by segment from checkpoints
- * every k iterations (the forward's, when nvb_set_checkpoints(h, k) preceded nvb_seed; else one
- * replay from the seed records them); adjoint vectors and dot products are FP64.  Needs
- * H^T = H (fails with NVB_ERR_STATE under quirk_lower with inter-state constant or even-power
- * couplings).  No reference counterpart (the reference has no derivative code). */
+ * nvb_hv_adjoint_coeffs.  Primal vectors are recomputed range by range, last range first, by
+ * replaying the recurrence from checkpoint pairs (v_{c-1}, v_c):
+ *   k > 0: one level, pairs every k iterations (the forward's, when nvb_set_checkpoints(h, k)
+ *          preceded nvb_seed; else one replay from the seed records them), each range of k
+ *          iterations replayed into storage (2k + 3 vectors of the handle's precision);
+ *   k = 0: automatic.  The shallowest recursion that fits the budget of
+ *          nvb_set_backward_memory (default 85% of free device memory): with depth L, each
+ *          level splits its range into B ~ n^(1/(L+1)) sub-ranges whose starting pairs one
+ *          replay records, down to ranges of at most B iterations replayed into storage
+ *          (2 L B + 2 B + 3 vectors; L + 1 replays of the run).  L = 0 (everything stored,
+ *          2n + 3 vectors) when it fits.  The forward's pairs, when recorded, are the top level.
+ * Adjoint vectors and dot products are FP64 in every plan; the gradient does not depend on the
+ * plan beyond rounding of FP64 sums.  Needs H^T = H (fails with NVB_ERR_STATE under
+ * quirk_lower with inter-state constant or even-power couplings).  No reference counterpart
+ * (the reference has no derivative code). */
 int nvb_lanczos_backward(nvb_handle *h, int64_t n, const double *alpha_bar, const double *beta_bar, int64_t k,
                          double *grad);
+
+/* Device-memory budget (bytes) of the automatic plan of nvb_lanczos_backward (k = 0); 0 = 85%
+ * of the free device memory at the call.  The sweep fails with NVB_ERR_NOMEM when even the
+ * deepest recursion does not fit.  No reference counterpart. */
+int nvb_set_backward_memory(nvb_handle *h, int64_t bytes);
+
+/* The last nvb_lanczos_backward's plan: plan[0] = interval of the top-level pairs (0 = the
+ * sweep started from the seed pair), plan[1] = branching B of a level, plan[2] = longest range
+ * replayed into storage, plan[3] = H.v applications spent in replays.  No reference
+ * counterpart. */
+int nvb_backward_plan(nvb_handle *h, int64_t *plan);
 
 /* <sa*a, sb*b> over the handle's total vector length (dimen*nstates) of two device vectors of
  * dtype, summed in FP64 in a fixed order (block partials in the handle's scratch, then one

@@ -59,6 +59,8 @@ _SIGS = {
     "nvb_convolve": [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_double, C.c_int64, C.c_void_p],
     "nvb_spin_orbit": [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p],
     "nvb_lanczos_backward": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p],
+    "nvb_set_backward_memory": [C.c_void_p, C.c_int64],
+    "nvb_backward_plan": [C.c_void_p, C.c_void_p],
     "nvb_get_terms": [C.c_void_p] + [C.c_void_p] * 7,
     "nvb_set_precision": [C.c_void_p, C.c_int64],
     "nvb_set_stream": [C.c_void_p, C.c_void_p],
@@ -347,8 +349,20 @@ class Handle:
         """Record (v_{c-1}, v_c) every k iterations from the next seed (nvb_set_checkpoints)."""
         check(lib().nvb_set_checkpoints(self.ptr, k))
 
-    def lanczos_backward(self, n: int, alpha_bar, beta_bar=None, k: int = 50) -> np.ndarray:
-        """dL/dtheta from dL/dalpha_1..n and dL/dbeta_1..n (nvb_lanczos_backward)."""
+    def set_backward_memory(self, nbytes: int):
+        """Device-memory budget of the automatic (k = 0) reverse sweep; 0 = 85% of free memory."""
+        check(lib().nvb_set_backward_memory(self.ptr, int(nbytes)))
+
+    def backward_plan(self) -> dict:
+        """The last reverse sweep's plan (nvb_backward_plan)."""
+        a = np.zeros(4, dtype=np.int64)
+        check(lib().nvb_backward_plan(self.ptr, _p(a)))
+        return {"top_interval": int(a[0]), "branching": int(a[1]), "stored_range": int(a[2]),
+                "replayed_hv": int(a[3])}
+
+    def lanczos_backward(self, n: int, alpha_bar, beta_bar=None, k: int = 0) -> np.ndarray:
+        """dL/dtheta from dL/dalpha_1..n and dL/dbeta_1..n (nvb_lanczos_backward); k = 0 picks
+        the checkpoint recursion from the memory budget, k > 0 is one level of interval k."""
         ab = np.ascontiguousarray(alpha_bar, dtype=np.float64)
         if ab.shape != (n,):
             raise ValueError("alpha_bar must have n entries")

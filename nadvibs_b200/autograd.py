@@ -7,8 +7,9 @@ code).
 file units), the block constants, then the frequencies (hartree).
 
 Forward: a handle is built from ``theta`` (``nvb_create``), seeded as the reference seeds
-(``Source/secondary.f90:727-783``), run for ``niter`` plain Lanczos iterations with
-checkpoints every ``k`` iterations, and T_n = tridiag(beta, alpha, beta) is diagonalised:
+(``Source/secondary.f90:727-783``), run for ``niter`` plain Lanczos iterations (recording
+checkpoint pairs every ``k`` iterations when k > 0), and T_n = tridiag(beta, alpha, beta) is
+diagonalised:
 Ritz energies E_i (hartree) and intensities I_i = s_{1,i}^2 (the squared first component of
 eigenvector i, the Franck-Condon weight of the seed, ``Source/secondary.f90:240-257``).
 
@@ -17,8 +18,10 @@ dL/dbeta_i,
     Tbar = S (diag(Ebar) + F o (S^T Sbar)) S^T,   F_ij = 1/(E_j - E_i) (i != j),
 with Sbar = e_1 (2 s_1 Ibar)^T; pairs of nearly equal Ritz values (ghost copies of a
 converged root) are damped, F_ij = d/(d^2 + eps^2).  Then ``nvb_lanczos_backward`` runs the
-reverse sweep through the recurrence on the GPU (segments recomputed from the checkpoints)
-and contracts the adjoint vectors with dH/dtheta.
+reverse sweep through the recurrence on the GPU and contracts the adjoint vectors with
+dH/dtheta.  The primal vectors are recomputed from checkpoint pairs: with k > 0 one level every
+k iterations; with k = 0 (the default) the shallowest recursive checkpointing that fits the
+device-memory budget (``Handle.set_backward_memory``; everything stored when it fits).
 """
 from __future__ import annotations
 
@@ -106,7 +109,7 @@ class LanczosRitz(torch.autograd.Function):
         return torch.from_numpy(g).to(ctx.dev), None, None, None, None
 
 
-def ritz(theta: torch.Tensor, params, niter: int, k: int = 50, **opts):
+def ritz(theta: torch.Tensor, params, niter: int, k: int = 0, **opts):
     """Differentiable Ritz energies (hartree) and intensities of niter Lanczos steps."""
     return LanczosRitz.apply(theta, params, niter, k, opts)
 

@@ -490,6 +490,21 @@ int nvb_set_checkpoints(nvb_handle *h, int64_t k) {
     });
 }
 
+int nvb_set_backward_memory(nvb_handle *h, int64_t bytes) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        if (bytes < 0) fail(NVB_ERR_ARG, "memory budget < 0");
+        h->grad_budget = bytes;
+    });
+}
+
+int nvb_backward_plan(nvb_handle *h, int64_t *plan) {
+    return guarded([&] {
+        if (!h || !plan) fail(NVB_ERR_ARG, "null argument");
+        for (int i = 0; i < 4; ++i) plan[i] = h->bw_plan[i];
+    });
+}
+
 int nvb_lanczos_backward(nvb_handle *h, int64_t n, const double *alpha_bar, const double *beta_bar, int64_t k,
                          double *grad) {
     return guarded([&] {

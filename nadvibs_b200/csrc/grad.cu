@@ -15,13 +15,16 @@
 // H^T = H: the reverse sweep refuses handles whose diagonal-section couplings are applied to
 // one triangle only (quirk_lower with constant or even-power inter-state couplings).
 //
-// The primal vectors come back segment by segment, last segment first: the forward saves
-// (v_{c-1}, v_c) every k iterations (nvb_set_checkpoints), and each segment of k iterations
-// is replayed from its checkpoint with the stored alpha/beta in the handle's precision, the
-// same way the two-pass Ritz vectors are rebuilt; the replay keeps v_j and w_j = H v_j of the
-// segment in FP64.  The adjoint vectors and every dot product are FP64.  Device memory:
-// 2 ceil(n/k) checkpoint vectors (handle precision) + (2k + 3) FP64 segment vectors + 6 FP64
-// work vectors.
+// The primal vectors come back range by range, last range first, by replaying the recurrence
+// with the stored alpha/beta in the handle's precision (the way the two-pass Ritz vectors are
+// rebuilt) from checkpoint pairs (v_{c-1}, v_c).  A range of at most bmax iterations is
+// replayed into storage (v_{c-1}..v_{e+1} and w_j = H v_j, native precision) and reversed; a
+// longer range is split into up to B sub-ranges, one replay records their starting pairs, and
+// they are reversed last-first (recursive checkpointing).  With an explicit interval k there is
+// one level: pairs every k iterations (the forward's, nvb_set_checkpoints) and bmax = k.  With
+// k = 0 the shallowest depth L that fits the memory budget is used (B = bmax ~ n^(1/(L+1)),
+// 2 L B + 2 bmax + 3 native vectors, L + 1 replays of the run).  The adjoint vectors and every
+// dot product are FP64 (10 FP64 work vectors).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -141,46 +144,6 @@ void ckpt_free(nvb_handle *h) {
 
 // ---------------------------------------------------------------- replay
 
-// Replays iterations from (prev = v_{c-1}, cur = v_c) in the handle's precision, writing the
-// FP64 vectors v_{c-1} .. v_{last} to seg[0 .. last-c+1] and w_j = H v_j (j = c .. last-1) to
-// wseg[0 .. last-c-1].  The three native buffers are scratch; the scales are host values.
-static void replay_segment(nvb_handle *h, void *b3[3], double sprev, double scur, int64_t c, int64_t last,
-                           double *seg, double *wseg, double *dsc) {
-    const long long N = h->ntotal();
-    const bool mixed = h->precision == NVB_MIXED;
-    const int dt = mixed ? NVB_DTYPE_F32 : NVB_DTYPE_F64;
-    int prev = 0, cur = 1, work = 2;
-    auto to64 = [&](double *dst, const void *src, double sc) {
-        if (mixed) k_to_f64<float><<<grid_g(N), 256, 0, h->stream>>>(dst, (const float *)src, sc, N);
-        else k_to_f64<double><<<grid_g(N), 256, 0, h->stream>>>(dst, (const double *)src, sc, N);
-    };
-    to64(seg, b3[prev], sprev);
-    for (int64_t j = c; j <= last; ++j) {
-        to64(seg + (size_t)(j - c + 1) * N, b3[cur], scur);
-        if (j == last) break;
-        CK(cudaMemcpyAsync(dsc, &scur, sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        hv_any(h, b3[cur], b3[work], dt, dsc, nullptr, nullptr);
-        to64(wseg + (size_t)(j - c) * N, b3[work], 1.0);  // w_j = H v_j, kept for the sweep
-        if (mixed)
-            k_replay<float><<<grid_g(N), 256, 0, h->stream>>>((float *)b3[work], (const float *)b3[cur],
-                                                              (const float *)b3[prev], scur, sprev, h->alpha[j],
-                                                              h->beta[j - 1], N);
-        else
-            k_replay<double><<<grid_g(N), 256, 0, h->stream>>>((double *)b3[work], (const double *)b3[cur],
-                                                               (const double *)b3[prev], scur, sprev, h->alpha[j],
-                                                               h->beta[j - 1], N);
-        CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(h->stream));  // dsc is rewritten next step
-        const int op = prev;
-        prev = cur;
-        cur = work;
-        work = op;
-        sprev = scur;
-        scur = 1.0 / h->beta[j];
-    }
-    CK(cudaStreamSynchronize(h->stream));
-}
-
 // The seed vector in native precision into buf (as lanczos_seed builds it); returns its scale.
 static double seed_native(nvb_handle *h, void *buf) {
     seed_fill(h, buf, seed_weights(h));
@@ -239,10 +202,178 @@ static void ckpt_by_replay(nvb_handle *h, int64_t k, int64_t n) {
 
 // ---------------------------------------------------------------- the reverse sweep
 
+namespace {
+
+// A checkpoint pair (v_{c-1}, v_c) in native buffers with their scales.
+struct CkPair {
+    const void *prev, *cur;
+    double sprev, scur;
+};
+
+struct Sweep {
+    nvb_handle *h = nullptr;
+    long long N = 0;
+    size_t per = 0, per64 = 0;
+    bool mixed = false;
+    int dt = NVB_DTYPE_F64, g = 1;
+    int64_t n = 0, B = 2, bmax = 1;  // branching of a level, longest range reversed from storage
+    void *b3[3] = {nullptr, nullptr, nullptr};
+    double *dsc = nullptr;
+    void *segv = nullptr, *segw = nullptr;  // native v_{c-1}..v_{e+1} and w_c..w_e of a base range
+    std::vector<double> segs;                // their scales
+    double *vb_next = nullptr, *vb_cur = nullptr, *vb_prev = nullptr, *rbar = nullptr, *wbar = nullptr,
+           *wv = nullptr, *v64[3] = {nullptr, nullptr, nullptr}, *w64 = nullptr;
+    std::vector<double> abar, bbar, gstep;
+    double *grad = nullptr;
+    int64_t nc = 0, replayed = 0;  // H.v applications of the replays
+
+    void to64(double *dst, const void *src, double sc) {
+        if (mixed) k_to_f64<float><<<g, 256, 0, h->stream>>>(dst, (const float *)src, sc, N);
+        else k_to_f64<double><<<g, 256, 0, h->stream>>>(dst, (const double *)src, sc, N);
+    }
+    void *nat(void *base, int64_t i) { return (char *)base + (size_t)i * per; }
+
+    // Replays iterations c..last from P: on_v(j, prev, sprev, cur, scur) at every j, and
+    // on_w(j, w) with w = H v_j (native) for j < last.
+    template <typename FV, typename FW>
+    void replay(const CkPair &P, int64_t c, int64_t last, FV on_v, FW on_w) {
+        CK(cudaMemcpyAsync(b3[0], P.prev, per, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(b3[1], P.cur, per, cudaMemcpyDeviceToDevice, h->stream));
+        int prev = 0, cur = 1, work = 2;
+        double sprev = P.sprev, scur = P.scur;
+        for (int64_t j = c; j <= last; ++j) {
+            on_v(j, b3[prev], sprev, b3[cur], scur);
+            if (j == last) break;
+            CK(cudaMemcpyAsync(dsc, &scur, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            hv_any(h, b3[cur], b3[work], dt, dsc, nullptr, nullptr);
+            ++replayed;
+            on_w(j, b3[work]);
+            if (mixed)
+                k_replay<float><<<g, 256, 0, h->stream>>>((float *)b3[work], (const float *)b3[cur],
+                                                          (const float *)b3[prev], scur, sprev, h->alpha[j],
+                                                          h->beta[j - 1], N);
+            else
+                k_replay<double><<<g, 256, 0, h->stream>>>((double *)b3[work], (const double *)b3[cur],
+                                                           (const double *)b3[prev], scur, sprev, h->alpha[j],
+                                                           h->beta[j - 1], N);
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(h->stream));  // dsc is rewritten next step
+            const int op = prev;
+            prev = cur;
+            cur = work;
+            work = op;
+            sprev = scur;
+            scur = 1.0 / h->beta[j];
+        }
+        CK(cudaStreamSynchronize(h->stream));
+    }
+
+    double dot(const double *a, const double *b) { return device_dot(h, a, 1.0, b, 1.0, NVB_DTYPE_F64); }
+
+    // reverse steps e..c of a range whose v_{c-1}..v_{e+1} and w_c..w_e are in segv/segw
+    void reverse_steps(int64_t c, int64_t e) {
+        auto V = [&](int64_t j, double *dst) { to64(dst, nat(segv, j - (c - 1)), segs[j - (c - 1)]); };
+        for (int64_t i = e; i >= c; --i) {
+            const double al = h->alpha[i], be = h->beta[i], bprev = h->beta[i - 1];
+            double *vn = v64[0], *vi = v64[1], *vp = v64[2];
+            V(i + 1, vn);
+            V(i, vi);
+            if (i > 1) V(i - 1, vp);
+            to64(w64, nat(segw, i - c), 1.0);  // w_i = H v_i from the replay
+            const double btot = bbar[i] - dot(vb_next, vn) / be;
+            k_lin<<<g, 256, 0, h->stream>>>(rbar, 1.0 / be, vb_next, btot, vn, 0, N);
+            const double atot = abar[i - 1] - dot(rbar, vi);
+            if (i > 1) bbar[i - 1] -= dot(rbar, vp);
+            k_lin<<<g, 256, 0, h->stream>>>(vb_cur, -al, rbar, atot, w64, 1, N);
+            k_lin<<<g, 256, 0, h->stream>>>(wbar, 1.0, rbar, atot, vi, 0, N);
+            if (i > 1) k_lin<<<g, 256, 0, h->stream>>>(vb_prev, -bprev, rbar, 0.0, nullptr, 1, N);
+            hv_any(h, wbar, wv, NVB_DTYPE_F64, nullptr, nullptr, nullptr);  // H wbar
+            k_lin<<<g, 256, 0, h->stream>>>(vb_cur, 1.0, wv, 0.0, nullptr, 1, N);
+            CK(cudaGetLastError());
+            hv_adjoint(h, wbar, vi, NVB_DTYPE_F64, gstep.data());
+            for (int64_t q = 0; q < nc; ++q) grad[q] += gstep[q];
+            // rotate: vbar_{i+1} <- vbar_i, vbar_i <- vbar_{i-1}, vbar_{i-1} <- 0
+            double *t = vb_next;
+            vb_next = vb_cur;
+            vb_cur = vb_prev;
+            vb_prev = t;
+            CK(cudaMemsetAsync(vb_prev, 0, per64, h->stream));
+        }
+    }
+
+    // Reverses iterations c..e given the pair at c.  Ranges up to bmax are replayed into the
+    // base storage; longer ones are split into up to B sub-ranges whose starting pairs one
+    // replay records, and reversed last-first.
+    void reverse_range(const CkPair &P, int64_t c, int64_t e) {
+        const int64_t len = e - c + 1;
+        if (len <= bmax) {
+            replay(
+                P, c, e + 1,
+                [&](int64_t j, const void *pv, double sp, const void *cv, double sc) {
+                    if (j == c) {
+                        CK(cudaMemcpyAsync(nat(segv, 0), pv, per, cudaMemcpyDeviceToDevice, h->stream));
+                        segs[0] = sp;
+                    }
+                    CK(cudaMemcpyAsync(nat(segv, j - c + 1), cv, per, cudaMemcpyDeviceToDevice, h->stream));
+                    segs[j - c + 1] = sc;
+                },
+                [&](int64_t j, const void *w) {
+                    CK(cudaMemcpyAsync(nat(segw, j - c), w, per, cudaMemcpyDeviceToDevice, h->stream));
+                });
+            reverse_steps(c, e);
+            return;
+        }
+        const int64_t sub = (len + B - 1) / B, nsub = (len + sub - 1) / sub;
+        DevBuf store(2 * (size_t)nsub * per);
+        std::vector<double> sc(2 * (size_t)nsub);
+        replay(
+            P, c, c + (nsub - 1) * sub,
+            [&](int64_t j, const void *pv, double sp, const void *cv, double scv) {
+                if ((j - c) % sub) return;
+                const int64_t t = (j - c) / sub;
+                CK(cudaMemcpyAsync(nat(store.p, 2 * t), pv, per, cudaMemcpyDeviceToDevice, h->stream));
+                CK(cudaMemcpyAsync(nat(store.p, 2 * t + 1), cv, per, cudaMemcpyDeviceToDevice, h->stream));
+                sc[2 * t] = sp;
+                sc[2 * t + 1] = scv;
+            },
+            [&](int64_t, const void *) {});
+        for (int64_t t = nsub - 1; t >= 0; --t) {
+            const CkPair Q{nat(store.p, 2 * t), nat(store.p, 2 * t + 1), sc[2 * t], sc[2 * t + 1]};
+            reverse_range(Q, c + t * sub, std::min(c + (t + 1) * sub - 1, e));
+        }
+    }
+};
+
+}  // namespace
+
+// Levels of the recursion for n iterations when `vectors` native vectors are available for
+// the pair stores and the base range: depth L (0 = one base range), branching B, base bmax.
+static bool plan_levels(int64_t n, double vectors, int64_t *L, int64_t *B, int64_t *bmax) {
+    for (int64_t l = 0; l <= 12; ++l) {
+        int64_t b = (int64_t)std::ceil(std::pow((double)n, 1.0 / (double)(l + 1)) - 1e-9);
+        b = std::max<int64_t>(b, 2);
+        while (b > 2) {  // the smallest b with b^(l+1) >= n
+            double p = 1.0;
+            for (int64_t q = 0; q <= l; ++q) p *= (double)(b - 1);
+            if (p >= (double)n) --b;
+            else break;
+        }
+        const int64_t base = l == 0 ? n : b;
+        const double need = 2.0 * (double)l * (double)b + 2.0 * (double)base + 3.0;
+        if (need <= vectors) {
+            *L = l;
+            *B = b;
+            *bmax = base;
+            return true;
+        }
+    }
+    return false;
+}
+
 void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const double *bbar_in, int64_t k,
                       double *grad) {
     if (n < 1 || n > h->iters) fail(NVB_ERR_ARG, "n must be in 1..iterations done");
-    if (k < 1) fail(NVB_ERR_ARG, "checkpoint interval must be >= 1");
+    if (k < 0) fail(NVB_ERR_ARG, "checkpoint interval must be >= 0 (0 = automatic from the memory budget)");
     if (h->reorthog > 0) fail(NVB_ERR_STATE, "the reverse sweep differentiates plain Lanczos (reorthog = 0)");
     if (!(h->beta[n] > 0.0)) fail(NVB_ERR_STATE, "beta_n is zero: v_{n+1} does not exist");
     {
@@ -253,65 +384,92 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
                     fail(NVB_ERR_STATE, "H is not symmetric (quirk_lower with inter-state constant or even-power "
                                         "couplings): the reverse sweep needs H^T = H");
     }
-    const long long N = h->ntotal();
-    const size_t per64 = (size_t)N * sizeof(double);
-    const size_t per = (size_t)N * h->elem_size();
-    const int64_t nc = ncoef_of(h);
-    // checkpoints: the forward's when they cover iterations 1..n with interval k, else replay
-    if (!(h->ck_k == k && h->ck_count >= (n + k - 1) / k && h->ck_buf)) ckpt_by_replay(h, k, n);
-    const int64_t nseg = (n + k - 1) / k;
-    std::vector<double> cks(2 * (size_t)nseg);
-    CK(cudaMemcpy(cks.data(), h->ck_scale, cks.size() * sizeof(double), cudaMemcpyDeviceToHost));
-
-    DevBuf segb((size_t)(k + 2) * per64), wsegb((size_t)(k + 1) * per64), b0(per), b1(per), b2(per),
+    Sweep W;
+    W.h = h;
+    W.n = n;
+    W.N = h->ntotal();
+    W.per = (size_t)W.N * h->elem_size();
+    W.per64 = (size_t)W.N * sizeof(double);
+    W.mixed = h->precision == NVB_MIXED;
+    W.dt = W.mixed ? NVB_DTYPE_F32 : NVB_DTYPE_F64;
+    W.g = grid_g(W.N);
+    W.nc = ncoef_of(h);
+    // the plan.  An explicit k is one level: pairs every k iterations (the forward's record, else
+    // one replay from the seed) and bmax = k.  k = 0 picks the shallowest recursion that fits the
+    // memory budget, over the forward's pairs when they were recorded, else from the seed.
+    int64_t top = 0;  // interval of the top-level pairs in h->ck_buf, 0 = start from the seed pair
+    if (k > 0) {
+        W.bmax = std::min(k, n);
+        W.B = (n + W.bmax - 1) / W.bmax;  // ranges of the one level
+        top = n > k ? k : 0;
+        if (top && !(h->ck_k == top && h->ck_count >= (n + top - 1) / top && h->ck_buf)) {
+            ckpt_by_replay(h, top, n);
+            W.replayed += n - 1;
+        }
+    } else {
+        const bool fwd = h->ck_k > 0 && h->ck_k < n && h->ck_buf && h->ck_count >= (n + h->ck_k - 1) / h->ck_k;
+        const int64_t span = fwd ? h->ck_k : n;
+        size_t freeb = 0, totalb = 0;
+        CK(cudaMemGetInfo(&freeb, &totalb));
+        const double budget = h->grad_budget > 0 ? (double)h->grad_budget : 0.85 * (double)freeb;
+        const double fixed = 5.0 * (double)W.per + 10.0 * (double)W.per64;
+        int64_t L = 0;
+        if (!plan_levels(span, (budget - fixed) / (double)W.per, &L, &W.B, &W.bmax))
+            fail(NVB_ERR_NOMEM, "the reverse sweep does not fit the device-memory budget");
+        top = fwd ? h->ck_k : 0;
+    }
+    h->bw_plan[0] = top;
+    h->bw_plan[1] = W.B;
+    h->bw_plan[2] = W.bmax;
+    // base storage and work vectors
+    DevBuf segv((size_t)(W.bmax + 2) * W.per), segw((size_t)(W.bmax + 1) * W.per), b0(W.per), b1(W.per), b2(W.per),
         dscb(sizeof(double));
-    DevBuf vbn(per64), vbc(per64), vbp(per64), rb(per64), wb(per64), w(per64);
-    double *seg = (double *)segb.p, *wseg = (double *)wsegb.p;
-    void *b3[3] = {b0.p, b1.p, b2.p};
-    double *vb_next = (double *)vbn.p, *vb_cur = (double *)vbc.p, *vb_prev = (double *)vbp.p;
-    double *rbar = (double *)rb.p, *wbar = (double *)wb.p, *wv = (double *)w.p;
-    CK(cudaMemsetAsync(vb_next, 0, per64, h->stream));
-    CK(cudaMemsetAsync(vb_cur, 0, per64, h->stream));
-    CK(cudaMemsetAsync(vb_prev, 0, per64, h->stream));
-    std::vector<double> abar(abar_in, abar_in + n), bbar(n + 1, 0.0);  // bbar[i] for beta_i, i = 0..n
-    for (int64_t i = 1; i <= n; ++i) bbar[i] = bbar_in ? bbar_in[i - 1] : 0.0;
-    std::fill(grad, grad + nc, 0.0);
-    std::vector<double> gstep(nc);
-    const int g = grid_g(N);
-    auto dot = [&](const double *a, const double *b) { return device_dot(h, a, 1.0, b, 1.0, NVB_DTYPE_F64); };
-
-    for (int64_t s = nseg - 1; s >= 0; --s) {
-        const int64_t c = 1 + s * k, e = std::min(c + k - 1, n);
-        // replay v_{c-1} .. v_{e+1} into seg[0 .. e-c+2]
-        CK(cudaMemcpyAsync(b3[0], (char *)h->ck_buf + 2 * (size_t)s * per, per, cudaMemcpyDeviceToDevice, h->stream));
-        CK(cudaMemcpyAsync(b3[1], (char *)h->ck_buf + (2 * (size_t)s + 1) * per, per, cudaMemcpyDeviceToDevice,
-                           h->stream));
-        replay_segment(h, b3, cks[2 * s], cks[2 * s + 1], c, e + 1, seg, wseg, (double *)dscb.p);
-        auto V = [&](int64_t j) { return seg + (size_t)(j - (c - 1)) * N; };  // v_j, c-1 <= j <= e+1
-        for (int64_t i = e; i >= c; --i) {
-            const double al = h->alpha[i], be = h->beta[i], bprev = h->beta[i - 1];
-            const double *wi = wseg + (size_t)(i - c) * N;  // w_i = H v_i from the replay
-            const double btot = bbar[i] - dot(vb_next, V(i + 1)) / be;
-            k_lin<<<g, 256, 0, h->stream>>>(rbar, 1.0 / be, vb_next, btot, V(i + 1), 0, N);
-            const double atot = abar[i - 1] - dot(rbar, V(i));
-            if (i > 1) bbar[i - 1] -= dot(rbar, V(i - 1));
-            k_lin<<<g, 256, 0, h->stream>>>(vb_cur, -al, rbar, atot, wi, 1, N);
-            k_lin<<<g, 256, 0, h->stream>>>(wbar, 1.0, rbar, atot, V(i), 0, N);
-            if (i > 1) k_lin<<<g, 256, 0, h->stream>>>(vb_prev, -bprev, rbar, 0.0, nullptr, 1, N);
-            hv_any(h, wbar, wv, NVB_DTYPE_F64, nullptr, nullptr, nullptr);  // H wbar
-            k_lin<<<g, 256, 0, h->stream>>>(vb_cur, 1.0, wv, 0.0, nullptr, 1, N);
-            CK(cudaGetLastError());
-            hv_adjoint(h, wbar, V(i), NVB_DTYPE_F64, gstep.data());
-            for (int64_t q = 0; q < nc; ++q) grad[q] += gstep[q];
-            // rotate: vbar_{i+1} <- vbar_i, vbar_i <- vbar_{i-1}, vbar_{i-1} <- 0
-            double *t = vb_next;
-            vb_next = vb_cur;
-            vb_cur = vb_prev;
-            vb_prev = t;
-            CK(cudaMemsetAsync(vb_prev, 0, per64, h->stream));
+    DevBuf vbn(W.per64), vbc(W.per64), vbp(W.per64), rb(W.per64), wb(W.per64), wvb(W.per64), c0(W.per64),
+        c1(W.per64), c2(W.per64), cw(W.per64);
+    W.segv = segv.p;
+    W.segw = segw.p;
+    W.segs.assign(W.bmax + 2, 0.0);
+    W.b3[0] = b0.p;
+    W.b3[1] = b1.p;
+    W.b3[2] = b2.p;
+    W.dsc = (double *)dscb.p;
+    W.vb_next = (double *)vbn.p;
+    W.vb_cur = (double *)vbc.p;
+    W.vb_prev = (double *)vbp.p;
+    W.rbar = (double *)rb.p;
+    W.wbar = (double *)wb.p;
+    W.wv = (double *)wvb.p;
+    W.v64[0] = (double *)c0.p;
+    W.v64[1] = (double *)c1.p;
+    W.v64[2] = (double *)c2.p;
+    W.w64 = (double *)cw.p;
+    CK(cudaMemsetAsync(W.vb_next, 0, W.per64, h->stream));
+    CK(cudaMemsetAsync(W.vb_cur, 0, W.per64, h->stream));
+    CK(cudaMemsetAsync(W.vb_prev, 0, W.per64, h->stream));
+    W.abar.assign(abar_in, abar_in + n);
+    W.bbar.assign(n + 1, 0.0);  // bbar[i] for beta_i, i = 0..n
+    for (int64_t i = 1; i <= n; ++i) W.bbar[i] = bbar_in ? bbar_in[i - 1] : 0.0;
+    W.grad = grad;
+    std::fill(grad, grad + W.nc, 0.0);
+    W.gstep.assign(W.nc, 0.0);
+    if (top == 0) {
+        // from the seed pair (v_0 = 0, v_1 = the seed)
+        DevBuf zero(W.per), seed(W.per);
+        CK(cudaMemsetAsync(zero.p, 0, W.per, h->stream));
+        seed_fill(h, seed.p, seed_weights(h));
+        W.reverse_range(CkPair{zero.p, seed.p, 0.0, 1.0 / h->beta[0]}, 1, n);
+    } else {
+        const int64_t nseg = (n + top - 1) / top;
+        std::vector<double> cks(2 * (size_t)nseg);
+        CK(cudaMemcpy(cks.data(), h->ck_scale, cks.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int64_t s2 = nseg - 1; s2 >= 0; --s2) {
+            const CkPair P{(char *)h->ck_buf + 2 * (size_t)s2 * W.per, (char *)h->ck_buf + (2 * (size_t)s2 + 1) * W.per,
+                         cks[2 * s2], cks[2 * s2 + 1]};
+            W.reverse_range(P, 1 + s2 * top, std::min((s2 + 1) * top, n));
         }
     }
     CK(cudaStreamSynchronize(h->stream));
+    h->bw_plan[3] = W.replayed;
     check_kernel_flags(h);
 }
 

@@ -52,6 +52,10 @@ struct nvb_handle {
     int64_t ck_k = 0, ck_count = 0, ck_cap = 0;
     void *ck_buf = nullptr;
     double *ck_scale = nullptr;
+    // the reverse sweep: device-memory budget for k = 0 (bytes, 0 = 85% of free memory) and
+    // the last sweep's plan (top-level interval, branching, longest stored range, replayed H.v)
+    int64_t grad_budget = 0;
+    int64_t bw_plan[4] = {0, 0, 0, 0};
     // displaced / Duschinsky seed: <m|n> over one state block (FP64) and its norm
     double *seed_vec = nullptr;
     double seed_norm = 0.0;

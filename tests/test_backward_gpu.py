@@ -93,6 +93,61 @@ def test_checkpoint_interval_and_recording_do_not_change_the_gradient():
         assert np.abs(g - ref).max() <= 1e-12 * scale, (k, rec)
 
 
+def _gradient_with_budget(p, theta, n, gE, gI, vectors, record_k=0, precision=None):
+    """Automatic plan (k = 0) under a budget of `vectors` vectors beyond the fixed work set."""
+    pot, cc, om = split_theta(theta, p.nstates, p.nmodes)
+    opts = {"quirk_lower": 0}
+    if precision is not None:
+        opts["precision"] = precision
+    with L.Handle.from_arrays(p, om, cc, pot, **opts) as h:
+        if record_k:
+            h.set_checkpoints(record_k)
+        h.seed()
+        a, b = h.lanczos(n)
+        E, S = tridiag_eigh(a[:n], b[1:n])
+        abar, bbar_off = tridiag_eig_backward(E, S, gE, gI)
+        bbar = np.zeros(n)
+        bbar[: n - 1] = bbar_off
+        N = p.nstates * int(np.prod([p.basis[i] for i in range(p.nmodes)]))
+        per = N * (4 if precision == L.NVB_MIXED else 8)
+        if vectors is not None:
+            h.set_backward_memory(int(5 * per + 10 * N * 8 + vectors * per))
+        g = h.lanczos_backward(n, abar, bbar, 0)
+        return g, h.backward_plan()
+
+
+@pytest.mark.parametrize("precision", [None, L.NVB_MIXED])
+def test_recursive_checkpointing_matches_single_level(precision):
+    """Depths 0, 1 and 2 of the automatic plan replay the same vectors as one level of interval
+    n, so the gradients agree to FP64 rounding; the plan follows the budget."""
+    p, theta = _system(80, 2, [4, 3, 3])
+    n = 40
+    rng = np.random.default_rng(80)
+    gE, gI = rng.normal(size=n), rng.normal(size=n)
+    opts = {"quirk_lower": 0}
+    if precision is not None:
+        opts["precision"] = precision
+    ref = _gradient(p, theta, n, gE, gI, k=n, record=False, **opts)
+    scale = np.abs(ref).max()
+    # vectors needed (2 L B + 2 B + 3): L = 0: 83, L = 1 (B = 7): 31, L = 2 (B = 4): 27
+    for vectors, branching, stored in [(None, n, n), (84, n, n), (32, 7, 7), (28, 4, 4)]:
+        g, plan = _gradient_with_budget(p, theta, n, gE, gI, vectors, precision=precision)
+        assert plan["top_interval"] == 0 and plan["stored_range"] == stored, (vectors, plan)
+        assert plan["branching"] == branching, (vectors, plan)
+        assert np.abs(g - ref).max() <= 1e-12 * scale, (vectors, plan)
+    # replays: depth 0 one pass (n - 1 H.v), depth 2 about three passes
+    _, p0 = _gradient_with_budget(p, theta, n, gE, gI, 84, precision=precision)
+    _, p2 = _gradient_with_budget(p, theta, n, gE, gI, 28, precision=precision)
+    assert p0["replayed_hv"] == n and 2 * n < p2["replayed_hv"] <= 3 * n, (p0, p2)
+    # the forward's recorded pairs become the top level
+    g, plan = _gradient_with_budget(p, theta, n, gE, gI, 32, record_k=10, precision=precision)
+    assert plan["top_interval"] == 10, plan
+    assert np.abs(g - ref).max() <= 1e-12 * scale
+    # below the deepest plan's need the sweep refuses instead of allocating
+    with pytest.raises(L.NvbError):
+        _gradient_with_budget(p, theta, n, gE, gI, 10, precision=precision)
+
+
 def test_converged_root_matches_hellmann_feynman():
     nstates, basis = 2, [5, 5, 3]
     p, theta = _system(75, nstates, basis)
@@ -206,7 +261,7 @@ def test_config4_spectrum_gradient_against_finite_differences():
     grid = torch.linspace(-200.0, 8000.0, 2048, dtype=torch.float64)
     w = torch.from_numpy(np.random.default_rng(4).normal(size=2048))
     th = torch.from_numpy(theta.copy()).requires_grad_(True)
-    E, I = ritz(th, p, n, k=50)
+    E, I = ritz(th, p, n)  # automatic checkpoint plan
     (w * convolved_spectrum(E, I, grid, 20.0)).sum().backward()
     g = th.grad.numpy()
     npot = theta.size - 3 - p.nmodes
