@@ -40,6 +40,7 @@ struct QuadArgs {
     int wait_limit;  // polls before a wait gives up
     long long dimen;
     unsigned dpm;
+    unsigned ownmask;  // bit a*S+b: the other state's own tile x_b is an item of target a
     QuadFast<T> F;
 };
 
@@ -104,7 +105,9 @@ __device__ __forceinline__ int item_row(int kind, int s) {
     return kind == QI_SLOW2 ? (s > 0 ? 2 : 3) : (s > 0 ? 0 : 1);
 }
 
-template <typename T, int S, int NF>
+// NC > 0: the number of consumer threads (= shft(m)) as a compile-time constant, so that the
+// rows of a thread's pencil are immediate offsets; NC = 0 reads it from the launch.
+template <typename T, int S, int NF, int NC>
 __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
     k_hv_quad(const QuadArgs<T> A, const T *__restrict__ x, T *__restrict__ y, const double *__restrict__ scale_dev,
               double *__restrict__ alpha_part) {
@@ -124,13 +127,13 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
     T *s_se = reinterpret_cast<T *>(smem + Lo.se);      // [2][MAXSL][5] slow element factors of a tile
     T *s_dt = reinterpret_cast<T *>(smem + Lo.dt);      // [2][S*S+1] slow diagonal block, energy
     QuadItem *s_it = reinterpret_cast<QuadItem *>(smem + Lo.items);
-    int *s_flag = reinterpret_cast<int *>(smem + Lo.flag);  // [2][nitems]
-    T *s_rec = reinterpret_cast<T *>(smem + Lo.rec);        // [2][nitems][NF+1]
+    int *s_cnt = reinterpret_cast<int *>(smem + Lo.cnt);  // [2][MAXS][2]
+    T *s_rec = reinterpret_cast<T *>(smem + Lo.rec);      // [2][nitems][NF+1]
     int *s_ib = reinterpret_cast<int *>(smem + Lo.items + A.nitems * (int)sizeof(QuadItem));
     T *s_ring = reinterpret_cast<T *>(smem + Lo.ring);  // [NS][sst]
     T *s_z = reinterpret_cast<T *>(smem + Lo.z);        // [NF-1][sst] Z_l, l > m
     const int tid = threadIdx.x;
-    const int nc = (int)blockDim.x - 32;  // consumer threads = shft(m)
+    const int nc = NC > 0 ? NC : (int)blockDim.x - 32;  // consumer threads = shft(m)
     const long long N = A.dimen;
     const QuadFast<T> &F = A.F;
     constexpr int SS = S * S;
@@ -155,7 +158,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
             s_sl[QUAD_MAXSL + i] = A.slow[m + i];
         }
         for (int i = tid; i < A.nitems; i += blockDim.x) s_it[i] = A.items[i];
-        for (int i = tid; i <= S; i += blockDim.x) s_ib[i] = A.item_beg[i];
+        for (int i = tid; i <= 3 * S; i += blockDim.x) s_ib[i] = A.item_beg[i];
         const int nz = (NS + (NF > 1 ? NF - 1 : 1)) * sst;  // ring and Z are contiguous
         for (int i = tid; i < nz; i += blockDim.x) s_ring[i] = (T)0;
     }
@@ -257,10 +260,26 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
     }
     const T sc = scale_dev ? (T)(*scale_dev) : (T)1;
     const int nv = A.nv;
+    const int lane = tid & 31, wid = tid >> 5;
     double part = 0.0;
     int slot = 0;
     unsigned ph = 0;
     int tp = 0;
+    bool ok = true;
+    // the next ring slot: wait for its copy (bounded), return this thread's column in it
+    auto take = [&]() -> const T * {
+        ok = mbar_try(&full[slot], ph) || mbar_wait(&full[slot], ph, abort_flag, A.wait_limit);
+        return s_ring + slot * sst + pad + tid;
+    };
+    // hand the slot back to the producer (one arrival per warp) and step to the next one
+    auto release = [&]() {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[slot]);
+        if (++slot == NS) {
+            slot = 0;
+            ph ^= 1u;
+        }
+    };
     for (int tile = blockIdx.x; tile < A.ntiles; tile += gridDim.x, tp ^= 1) {
         // the tile's slow element factors and the slow part of the diagonal block
         if (tid < m) {
@@ -289,35 +308,30 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
         consumer_sync(nc);
         const T *se = s_se + tp * QUAD_MAXSL * 5;
         const T *dt = s_dt + tp * (SS + 1);
-        // item records of the tile: flag (0 absent, 1 neighbour, 2 neighbour feeding Z,
-        // 3 own tile, 4 another state's own tile) and coefficients c, z[j] with the slow
-        // element factors folded in
-        {
-            int *fl = s_flag + tp * A.nitems;
-            T *rc = s_rec + tp * A.nitems * (NF + 1);
-            for (int i = tid; i < A.nitems; i += nc) {
-                const QuadItem q = s_it[i];
-                const int a = q.a, b = q.b;
-                int f;
+        // records of the tile's present slow items, compacted per target state a by one
+        // consumer warp (warp a mod the consumer warps) in the producer's order: coefficient c and z[j] with the slow element factors folded in
+        // (z only for the Z items, which come first); the counts go to s_cnt
+        for (int a = wid; a < S; a += nc >> 5) {  // nc >= 64: at least two consumer warps
+            const int beg = s_ib[S + 1 + a], zend = s_ib[2 * S + 1 + a], end = s_ib[a + 1];
+            T *rc = s_rec + (tp * A.nitems + s_ib[a]) * (NF + 1);
+            int base = 0, nzp = 0;
+            for (int i0 = beg; i0 < end; i0 += 32) {
+                const int i = i0 + lane;
+                bool present = false;
                 T c = (T)0, z[NF];
 #pragma unroll
                 for (int j = 0; j < NF; ++j) z[j] = (T)0;
-                if (q.kind == QI_OWN) {
-                    f = b == a ? 3 : 4;
-                } else {
+                if (i < end) {
+                    const QuadItem q = s_it[i];
+                    const int b = q.b;
                     T e = se[q.k * 5 + item_row(q.kind, q.sk)];
                     if (q.kind == QI_PAIR) e *= se[q.l * 5 + item_row(q.kind, q.sl)];
-                    f = e != (T)0 ? 1 : 0;
+                    present = e != (T)0;
                     if (q.kind == QI_SLOW1) {
                         c = s_G[q.k * SS + a * S + b] * e;
-                        if (b == a) {
-                            bool any = false;
+                        if (i < zend) {
 #pragma unroll
-                            for (int j = 0; j < NF; ++j) {
-                                z[j] = s_Q[(q.k * M + m + j) * S + a] * e;
-                                any |= z[j] != (T)0;
-                            }
-                            if (any && f) f = 2;
+                            for (int j = 0; j < NF; ++j) z[j] = s_Q[(q.k * M + m + j) * S + a] * e;
                         }
                     } else if (q.kind == QI_SLOW2) {
                         c = s_R[q.k * SS + a * S + b] * e;
@@ -325,15 +339,23 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                         c = s_Q[(q.k * M + q.l) * S + a] * e;
                     }
                 }
-                fl[i] = f;
-                rc[i * (NF + 1)] = c;
+                const unsigned bal = __ballot_sync(0xffffffffu, present);
+                const unsigned balz = __ballot_sync(0xffffffffu, present && i < zend);
+                if (present) {
+                    const int pos = base + __popc(bal & ((1u << lane) - 1u));
+                    rc[pos * (NF + 1)] = c;
 #pragma unroll
-                for (int j = 0; j < NF; ++j) rc[i * (NF + 1) + 1 + j] = z[j];
+                    for (int j = 0; j < NF; ++j) rc[pos * (NF + 1) + 1 + j] = z[j];
+                }
+                base += __popc(bal);
+                nzp += __popc(balz);
+            }
+            if (lane == 0) {
+                s_cnt[(tp * QUAD_MAXS + a) * 2] = nzp;
+                s_cnt[(tp * QUAD_MAXS + a) * 2 + 1] = base;
             }
         }
         consumer_sync(nc);
-        const int *fl = s_flag + tp * A.nitems;
-        const T *rc = s_rec + tp * A.nitems * (NF + 1);
         const long long tbase = (long long)tile * TF;
 #pragma unroll
         for (int a = 0; a < S; ++a) {
@@ -347,85 +369,111 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
             T hj[NF];  // <n|x^2|n> of the thread's fast digits (j >= 1)
 #pragma unroll
             for (int j = 0; j < NF; ++j) hj[j] = (T)dj[j] + (T)0.5;
-            const int iend = s_ib[a + 1];
-            for (int it = s_ib[a]; it < iend; ++it) {
-                const int f = fl[it];
-                if (f == 0) continue;
-                const bool ok = mbar_try(&full[slot], ph) || mbar_wait(&full[slot], ph, abort_flag, A.wait_limit);
-                const T *buf = s_ring + slot * sst + pad;
+            // own tile x_a: diagonal section, fast linear and bilinear into Z, fast squares
+            {
+                const T *buf = take();
                 if (ok) {
-                    if (f <= 2) {
-                        T v[R];
 #pragma unroll
-                        for (int r = 0; r < R; ++r) v[r] = buf[r * nc + tid];
-                        const T c = rc[it * (NF + 1)];
+                    for (int r = 0; r < R; ++r) xr[r] = buf[r * nc];
+                    T ek = dt[SS], daa = dt[a * S + a];
 #pragma unroll
-                        for (int r = 0; r < R; ++r) acc[r] += c * v[r];
-                        if (f == 2) {
+                    for (int j = 1; j < NF; ++j) {
+                        ek += F.om[j] * hj[j];
+                        daa += F.R[j][a][a] * hj[j];
+                    }
 #pragma unroll
-                            for (int j = 0; j < NF; ++j) {
-                                const T zq = rc[it * (NF + 1) + 1 + j];
+                    for (int r = 0; r < R; ++r) {
+                        const T h = (T)r + (T)0.5;
+                        acc[r] += (daa + F.R[0][a][a] * h + ek + F.om[0] * h) * xr[r];
+                    }
 #pragma unroll
-                                for (int r = 0; r < R; ++r) Z[j][r] += zq * v[r];
+                    for (int j = 0; j < NF; ++j) {
+                        const T g = F.G[j][a][a];
+                        if (g != (T)0) {
+#pragma unroll
+                            for (int r = 0; r < R; ++r) Z[j][r] += g * xr[r];
+                        }
+                    }
+                    // Z_l += Q^a_il X_i x_a (fast i < l)
+#pragma unroll
+                    for (int i = 0; i + 1 < NF; ++i) {
+                        bool any = false;
+#pragma unroll
+                        for (int j = i + 1; j < NF; ++j) any |= F.Q[i][j][a] != (T)0;
+                        if (!any) continue;
+                        T V[R];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            if (i == 0) {
+                                T v = (T)0;
+                                if (r + 1 < R) v += F.em[0][r] * xr[r + 1];
+                                if (r >= 1) v += F.em[1][r] * xr[r - 1];
+                                V[r] = v;
+                            } else {
+                                const T *p = buf + r * nc;
+                                V[r] = e1p[i] * p[F.sh[i]] + e1m[i] * p[-F.sh[i]];
                             }
                         }
-                    } else if (f == 3) {
 #pragma unroll
-                        for (int r = 0; r < R; ++r) xr[r] = buf[r * nc + tid];
-                        // diagonal section
-                        T ek = dt[SS], daa = dt[a * S + a];
+                        for (int j = i + 1; j < NF; ++j) {
+                            const T qq = F.Q[i][j][a];
+                            if (qq == (T)0) continue;
 #pragma unroll
-                        for (int j = 1; j < NF; ++j) {
-                            ek += F.om[j] * hj[j];
-                            daa += F.R[j][a][a] * hj[j];
+                            for (int r = 0; r < R; ++r) Z[j][r] += qq * V[r];
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < NF; ++j) {
+                        const T rr = F.R[j][a][a];
+                        if (rr == (T)0) continue;
+                        T e2p = (T)0, e2m = (T)0;
+                        if (j >= 1) {
+                            e2p = s_tab[((m + j) * 5 + 2) * nmax + dj[j]];
+                            e2m = s_tab[((m + j) * 5 + 3) * nmax + dj[j]];
                         }
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
-                            const T h = (T)r + (T)0.5;
-                            acc[r] += (daa + F.R[0][a][a] * h + ek + F.om[0] * h) * xr[r];
-                        }
-                        // fast linear, own state
-#pragma unroll
-                        for (int j = 0; j < NF; ++j) {
-                            const T g = F.G[j][a][a];
-                            if (g != (T)0) {
-#pragma unroll
-                                for (int r = 0; r < R; ++r) Z[j][r] += g * xr[r];
+                            T v = (T)0;
+                            if (j == 0) {
+                                if (r + 2 < R) v += F.em[2][r] * xr[r + 2];
+                                if (r >= 2) v += F.em[3][r] * xr[r - 2];
+                            } else {
+                                const T *p = buf + r * nc;
+                                v = e2p * p[2 * F.sh[j]] + e2m * p[-2 * F.sh[j]];
                             }
+                            acc[r] += rr * v;
                         }
-                        // fast bilinear: Z_l += Q^a_il X_i x_a (fast i < l)
+                    }
+                }
+                release();
+            }
+            // the other states' own tiles x_b: diagonal-section entries, fast linear into Z,
+            // fast squares
 #pragma unroll
-                        for (int i = 0; i + 1 < NF; ++i) {
-                            bool any = false;
+            for (int b = 0; b < S; ++b) {
+                if (b == a || !((A.ownmask >> (a * S + b)) & 1u)) continue;
+                const T *buf = take();
+                if (ok) {
+                    T xb[R];
 #pragma unroll
-                            for (int j = i + 1; j < NF; ++j) any |= F.Q[i][j][a] != (T)0;
-                            if (!any) continue;
-                            T V[R];
+                    for (int r = 0; r < R; ++r) xb[r] = buf[r * nc];
+                    if ((A.dpm >> (a * S + b)) & 1u) {
+                        T dab = dt[a * S + b];
 #pragma unroll
-                            for (int r = 0; r < R; ++r) {
-                                if (i == 0) {
-                                    T v = (T)0;
-                                    if (r + 1 < R) v += F.em[0][r] * xr[r + 1];
-                                    if (r >= 1) v += F.em[1][r] * xr[r - 1];
-                                    V[r] = v;
-                                } else {
-                                    const T *p = buf + r * nc + tid;
-                                    V[r] = e1p[i] * p[F.sh[i]] + e1m[i] * p[-F.sh[i]];
-                                }
-                            }
+                        for (int j = 1; j < NF; ++j) dab += F.R[j][a][b] * hj[j];
+                        const T r0 = F.R[0][a][b];
 #pragma unroll
-                            for (int j = i + 1; j < NF; ++j) {
-                                const T qq = F.Q[i][j][a];
-                                if (qq == (T)0) continue;
+                        for (int r = 0; r < R; ++r) acc[r] += (dab + r0 * ((T)r + (T)0.5)) * xb[r];
+                    }
 #pragma unroll
-                                for (int r = 0; r < R; ++r) Z[j][r] += qq * V[r];
-                            }
+                    for (int j = 0; j < NF; ++j) {
+                        const T g = F.G[j][a][b];
+                        if (g != (T)0) {
+#pragma unroll
+                            for (int r = 0; r < R; ++r) Z[j][r] += g * xb[r];
                         }
-                        // fast squares, own state
-#pragma unroll
-                        for (int j = 0; j < NF; ++j) {
-                            const T rr = F.R[j][a][a];
-                            if (rr == (T)0) continue;
+                        const T rr = F.R[j][a][b];
+                        if (rr != (T)0) {
                             T e2p = (T)0, e2m = (T)0;
                             if (j >= 1) {
                                 e2p = s_tab[((m + j) * 5 + 2) * nmax + dj[j]];
@@ -434,65 +482,78 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
 #pragma unroll
                             for (int r = 0; r < R; ++r) {
                                 T v = (T)0;
+                                const T *p = buf + r * nc;
                                 if (j == 0) {
-                                    if (r + 2 < R) v += F.em[2][r] * xr[r + 2];
-                                    if (r >= 2) v += F.em[3][r] * xr[r - 2];
+                                    if (r + 2 < R) v += F.em[2][r] * p[2 * nc];
+                                    if (r >= 2) v += F.em[3][r] * p[-2 * nc];
                                 } else {
-                                    const T *p = buf + r * nc + tid;
                                     v = e2p * p[2 * F.sh[j]] + e2m * p[-2 * F.sh[j]];
                                 }
                                 acc[r] += rr * v;
                             }
                         }
-                    } else {
-                        // another state's own tile
-                        const int b = s_it[it].b;
-                        T xb[R];
-#pragma unroll
-                        for (int r = 0; r < R; ++r) xb[r] = buf[r * nc + tid];
-                        if ((A.dpm >> (a * S + b)) & 1u) {
-                            T dab = dt[a * S + b];
-#pragma unroll
-                            for (int j = 1; j < NF; ++j) dab += F.R[j][a][b] * hj[j];
-                            const T r0 = F.R[0][a][b];
-#pragma unroll
-                            for (int r = 0; r < R; ++r) acc[r] += (dab + r0 * ((T)r + (T)0.5)) * xb[r];
-                        }
-#pragma unroll
-                        for (int j = 0; j < NF; ++j) {
-                            const T g = F.G[j][a][b];
-                            if (g != (T)0) {
-#pragma unroll
-                                for (int r = 0; r < R; ++r) Z[j][r] += g * xb[r];
-                            }
-                            const T rr = F.R[j][a][b];
-                            if (rr != (T)0) {
-                                T e2p = (T)0, e2m = (T)0;
-                                if (j >= 1) {
-                                    e2p = s_tab[((m + j) * 5 + 2) * nmax + dj[j]];
-                                    e2m = s_tab[((m + j) * 5 + 3) * nmax + dj[j]];
-                                }
-#pragma unroll
-                                for (int r = 0; r < R; ++r) {
-                                    T v = (T)0;
-                                    const T *p = buf + r * nc + tid;
-                                    if (j == 0) {
-                                        if (r + 2 < R) v += F.em[2][r] * p[2 * nc];
-                                        if (r >= 2) v += F.em[3][r] * p[-2 * nc];
-                                    } else {
-                                        v = e2p * p[2 * F.sh[j]] + e2m * p[-2 * F.sh[j]];
-                                    }
-                                    acc[r] += rr * v;
-                                }
-                            }
-                        }
                     }
                 }
-                __syncwarp();
-                if ((tid & 31) == 0) mbar_arrive(&empty[slot]);
-                if (++slot == NS) {
-                    slot = 0;
-                    ph ^= 1u;
+                release();
+            }
+            // present slow items: the Z items (y_a += c x, Z_l += z_l x), then the
+            // coefficient-only items two at a time
+            {
+                const int nzp = s_cnt[(tp * QUAD_MAXS + a) * 2], nsp = s_cnt[(tp * QUAD_MAXS + a) * 2 + 1];
+                const T *rc = s_rec + (tp * A.nitems + s_ib[a]) * (NF + 1);
+                int j = 0;
+                for (; j < nzp; ++j) {
+                    const T *buf = take();
+                    if (ok) {
+                        T v[R];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) v[r] = buf[r * nc];
+                        const T c = rc[j * (NF + 1)];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) acc[r] += c * v[r];
+#pragma unroll
+                        for (int q = 0; q < NF; ++q) {
+                            const T zq = rc[j * (NF + 1) + 1 + q];
+#pragma unroll
+                            for (int r = 0; r < R; ++r) Z[q][r] += zq * v[r];
+                        }
+                    }
+                    release();
+                }
+                for (; j + 1 < nsp; j += 2) {
+                    // two consecutive slots: the first is held (not released) while the second
+                    // is awaited; the ring has at least three slots
+                    const T *b0 = take();
+                    const bool ok0 = ok;
+                    const int s0 = slot;
+                    if (++slot == NS) {
+                        slot = 0;
+                        ph ^= 1u;
+                    }
+                    const T *b1 = take();
+                    if (ok0 && ok) {
+                        T v0[R], v1[R];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            v0[r] = b0[r * nc];
+                            v1[r] = b1[r * nc];
+                        }
+                        const T c0 = rc[j * (NF + 1)], c1 = rc[(j + 1) * (NF + 1)];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) acc[r] += c0 * v0[r] + c1 * v1[r];
+                    }
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&empty[s0]);
+                    release();
+                }
+                if (j < nsp) {
+                    const T *buf = take();
+                    if (ok) {
+                        const T c = rc[j * (NF + 1)];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) acc[r] += c * buf[r * nc];
+                    }
+                    release();
                 }
             }
             // y_a += X_l Z_l
@@ -559,6 +620,7 @@ QuadArgs<T> quad_args(const QuadPlan &qp) {
     a.nitems = (int)qp.items.size();
     a.dimen = qp.dimen;
     a.dpm = qp.dpm;
+    a.ownmask = qp.ownmask;
     if constexpr (sizeof(T) == 8) {
         a.blk = (const T *)qp.d_blk;
         a.F = qp.fast_d;
@@ -571,12 +633,12 @@ QuadArgs<T> quad_args(const QuadPlan &qp) {
     return a;
 }
 
-template <typename T, int S, int NF>
+template <typename T, int S, int NF, int NC>
 int launch_q(QuadPlan &qp, const T *x, T *y, const double *sc, double *ap, cudaStream_t st) {
     const int idx = sizeof(T) == 8 ? 0 : 1;
     const size_t smem = qp.smem[idx];
     const int threads = qp.threads + 32;
-    auto kern = k_hv_quad<T, S, NF>;
+    auto kern = k_hv_quad<T, S, NF, NC>;
     if (qp.grid[idx] == 0) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int dev = 0, nsm = 0, per = 0;
@@ -594,10 +656,11 @@ int launch_q(QuadPlan &qp, const T *x, T *y, const double *sc, double *ap, cudaS
 
 template <typename T, int S>
 int launch_qs(QuadPlan &qp, const T *x, T *y, const double *sc, double *ap, cudaStream_t st) {
+    const bool n288 = qp.threads == 288;
     switch (qp.nF) {
-    case 2: return launch_q<T, S, 2>(qp, x, y, sc, ap, st);
-    case 3: return launch_q<T, S, 3>(qp, x, y, sc, ap, st);
-    case 4: return launch_q<T, S, 4>(qp, x, y, sc, ap, st);
+    case 2: return n288 ? launch_q<T, S, 2, 288>(qp, x, y, sc, ap, st) : launch_q<T, S, 2, 0>(qp, x, y, sc, ap, st);
+    case 3: return n288 ? launch_q<T, S, 3, 288>(qp, x, y, sc, ap, st) : launch_q<T, S, 3, 0>(qp, x, y, sc, ap, st);
+    case 4: return n288 ? launch_q<T, S, 4, 288>(qp, x, y, sc, ap, st) : launch_q<T, S, 4, 0>(qp, x, y, sc, ap, st);
     default: fail(NVB_ERR_ARG, "quadratic kernel: unsupported number of fast modes");
     }
 }

@@ -73,8 +73,12 @@ struct QuadPlan {
     std::vector<double> tab;  // per mode j: rows E1+, E1-, E2+, E2-, D2, each of nmax
     std::vector<double> omega;
     std::vector<int> slow_tshft, slow_nfunc;
-    std::vector<QuadItem> items;  // per target state a: items[item_beg[a] .. item_beg[a+1])
-    std::vector<int> item_beg;
+    // per target state a: items[item_beg[a] .. item_beg[a+1]) in the order own a, the other
+    // states' own tiles (bit a*S+b of ownmask), from slow_beg[a] the slow +-1 tiles of state a
+    // that feed Z (up to z_end[a]), then the coefficient-only slow items
+    std::vector<QuadItem> items;
+    std::vector<int> item_beg, slow_beg, z_end;
+    unsigned ownmask = 0;
     int nslot[2] = {0, 0};        // ring slots, FP64 / FP32
     QuadFast<double> fast_d{};
     QuadFast<float> fast_f{};
@@ -92,7 +96,7 @@ struct QuadPlan {
 
 // Shared-memory layout (byte offsets), identical on host and device.
 struct QuadLayout {
-    int tab, G, R, Q, cst, om, sd, se, dt, items, flag, rec, ring, z, total;
+    int tab, G, R, Q, cst, om, sd, se, dt, items, cnt, rec, ring, z, total;
 };
 constexpr int QUAD_MAXSLOT = 16;
 __host__ __device__ inline QuadLayout quad_layout(int M, int S, int nmax, int m, int nF, int sstate, int eb,
@@ -113,9 +117,9 @@ __host__ __device__ inline QuadLayout quad_layout(int M, int S, int nmax, int m,
     L.sd = take(2 * QUAD_MAXSL * 4);
     L.se = take(2 * QUAD_MAXSL * 5 * eb);
     L.dt = take(2 * (S * S + 1) * eb);
-    L.items = take(nitems * (int)sizeof(QuadItem) + (S + 1) * 4);
-    L.flag = take(2 * nitems * 4);                  // per tile parity: item flags
-    L.rec = take(2 * nitems * (nF + 1) * eb);       // per tile parity: c, z[nF] of each item
+    L.items = take(nitems * (int)sizeof(QuadItem) + (3 * QUAD_MAXS + 1) * 4);
+    L.cnt = take(2 * QUAD_MAXS * 2 * 4);            // per tile parity and target: Z items, slow items present
+    L.rec = take(2 * nitems * (nF + 1) * eb);       // per tile parity: c, z[nF] of the present slow items
     o = (o + 127) / 128 * 128;
     L.ring = take(nslot * sstate * eb);
     L.z = take((nF > 1 ? nF - 1 : 1) * sstate * eb);

@@ -120,6 +120,9 @@ bool quad_build(QuadPlan &qp, const Plan &pl, const System &sys) {
     // ring items per target state: own tiles, slow +-1, slow +-2, slow bilinear
     qp.items.clear();
     qp.item_beg.assign(S + 1, 0);
+    qp.slow_beg.assign(S, 0);
+    qp.z_end.assign(S, 0);
+    qp.ownmask = 0;
     for (int a = 0; a < S; ++a) {
         qp.item_beg[a] = (int)qp.items.size();
         auto push = [&](int kind, int b, int k, int sk, int l, int sl) {
@@ -144,15 +147,30 @@ bool quad_build(QuadPlan &qp, const Plan &pl, const System &sys) {
             }
             for (int j = 0; j < qp.nF; ++j)
                 need |= qp.G[((size_t)(m + j) * S + a) * S + b] != 0.0 || qp.R[((size_t)(m + j) * S + a) * S + b] != 0.0;
-            if (need) push(QI_OWN, b, 0, 0, 0, 0);
+            if (need) {
+                push(QI_OWN, b, 0, 0, 0, 0);
+                qp.ownmask |= 1u << (a * S + b);
+            }
         }
+        // slow +-1: first the own state's tiles that feed Z (slow-fast bilinear), then the
+        // coefficient-only ones, so that the kernel's per-tile records keep the Z items first
+        qp.slow_beg[a] = (int)qp.items.size();
+        auto feeds_z = [&](int k) {
+            for (int j = 0; j < qp.nF; ++j)
+                if (qp.Q[((size_t)k * M + m + j) * S + a] != 0.0) return true;
+            return false;
+        };
+        for (int k = 0; k < m; ++k)
+            if (sys.nfunc[k] >= 2 && feeds_z(k)) {
+                push(QI_SLOW1, a, k, +1, 0, 0);
+                push(QI_SLOW1, a, k, -1, 0, 0);
+            }
+        qp.z_end[a] = (int)qp.items.size();
         for (int k = 0; k < m; ++k) {
             if (sys.nfunc[k] < 2) continue;
             for (int b = 0; b < S; ++b) {
-                bool need = qp.G[((size_t)k * S + a) * S + b] != 0.0;
-                if (b == a)
-                    for (int j = 0; j < qp.nF; ++j) need |= qp.Q[((size_t)k * M + m + j) * S + a] != 0.0;
-                if (!need) continue;
+                if (b == a && feeds_z(k)) continue;
+                if (qp.G[((size_t)k * S + a) * S + b] == 0.0) continue;
                 push(QI_SLOW1, b, k, +1, 0, 0);
                 push(QI_SLOW1, b, k, -1, 0, 0);
             }
@@ -211,8 +229,12 @@ void quad_upload(QuadPlan &qp) {
     CK(cudaMemcpy(qp.d_slow, slow.data(), slow.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&qp.d_items, qp.items.size() * sizeof(QuadItem)));
     CK(cudaMemcpy(qp.d_items, qp.items.data(), qp.items.size() * sizeof(QuadItem), cudaMemcpyHostToDevice));
-    CK(cudaMalloc((void **)&qp.d_item_beg, qp.item_beg.size() * sizeof(int)));
-    CK(cudaMemcpy(qp.d_item_beg, qp.item_beg.data(), qp.item_beg.size() * sizeof(int), cudaMemcpyHostToDevice));
+    // item_beg[0..S], slow_beg[0..S-1], z_end[0..S-1]
+    std::vector<int> beg(qp.item_beg);
+    beg.insert(beg.end(), qp.slow_beg.begin(), qp.slow_beg.end());
+    beg.insert(beg.end(), qp.z_end.begin(), qp.z_end.end());
+    CK(cudaMalloc((void **)&qp.d_item_beg, beg.size() * sizeof(int)));
+    CK(cudaMemcpy(qp.d_item_beg, beg.data(), beg.size() * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void **)&qp.d_err, sizeof(int)));
     CK(cudaMemset(qp.d_err, 0, sizeof(int)));
 }
