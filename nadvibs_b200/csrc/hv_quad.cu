@@ -1,13 +1,13 @@
 // Factorised quadratic H.v kernel (see quad.h for the algebra).
 //
 // Warp-specialised persistent CTAs walk the tiles (fixed slow digits) with a stride of the
-// grid.  The last warp is the producer: one lane walks the same item sequence as the
-// consumers (per tile, per target state a: the own tile x_a, the other states' own tiles,
-// the slow +-1 / +-2 / bilinear neighbour tiles) and copies each valid item into the next
-// slot of a ring of shared-memory buffers with a TMA bulk copy completing on the slot's
-// "full" mbarrier, after the consumers released the slot on its "empty" mbarrier.  The other
-// warps are the consumers; a thread owns the pencil of mode m (rows r*shft(m) + tid) and
-// folds each item into registers:
+// grid.  The last warp is the producer: it lists each tile's valid items one tile ahead, and
+// one lane walks the same item sequence as the consumers (per tile, per target state a: the
+// own tile x_a, the other states' own tiles, the slow +-1 / +-2 / bilinear neighbour tiles),
+// copying each item into the next slot of a ring of shared-memory buffers with a TMA bulk
+// copy completing on the slot's "full" mbarrier, after the consumers released the slot on its
+// "empty" mbarrier.  The other warps are the consumers; a thread owns the pencil of mode m
+// (rows r*shft(m) + tid) and folds each item into registers:
 //   own x_a:      diagonal section, Z_l += G^aa_l x_a + Q^a_kl X_k x_a (fast k < l), squares;
 //   own x_b:      off-diagonal diagonal-section entries, Z_l += G^ab_l x_b, squares of x_b;
 //   slow +-1:     y_a += G^ab_k e x_b(p+-e_k), Z_l += Q^a_kl e x_a(p+-e_k);
@@ -175,52 +175,62 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
 
     if (tid >= nc) {
         // ---------------- producer ----------------
-        // Per tile the warp evaluates which items exist (one bit per item, 32 items per
-        // ballot, word w kept by lane w); lane 0 then issues the copies in item order.
+        // One tile ahead of the copies the warp lists the tile's present items (ballot per 32
+        // items, compacted into s_pl[q] for tile parity q, count first); lane 0 then issues
+        // the tile's copies from the list in consumption order, each after its slot was
+        // released.  (Listing ahead keeps the ballots out of the gap between two tiles' copies;
+        // one issuing lane keeps the copies in the order the consumers take them, which
+        // measured faster than one lane per slot.)
         const int lane = tid - nc;
         const unsigned bytes = (unsigned)TF * (unsigned)sizeof(T);
         const int nit = s_ib[S];
-        const int nw = (nit + 31) >> 5;  // <= 32 words: nitems <= 1024
-        int slot = 0;
-        unsigned ph = 0;
-        long long issued = 0;
-        int stop = A.nocopy;
-        for (int tile = blockIdx.x; tile < A.ntiles && !stop; tile += gridDim.x) {
-            unsigned myw = 0;
-            for (int w = 0; w < nw; ++w) {
-                const int it = (w << 5) + lane;
+        int *s_pl = reinterpret_cast<int *>(smem + Lo.plist);  // [2][nitems + 1]
+        auto list = [&](int tile, int q) {
+            int *pl = s_pl + q * (nit + 1);
+            int base = 0;
+            for (int i0 = 0; i0 < nit; i0 += 32) {
+                const int it = i0 + lane;
                 bool ok = false;
                 if (it < nit) {
-                    const QuadItem q = s_it[it];
+                    const QuadItem qi = s_it[it];
                     ok = true;
-                    if (q.kind != QI_OWN) {
-                        const int dk = (tile / tsh[q.k]) % snf[q.k];
-                        ok = s_tab[(q.k * 5 + item_row(q.kind, q.sk)) * nmax + dk] != (T)0;
-                        if (q.kind == QI_PAIR) {
-                            const int dl = (tile / tsh[q.l]) % snf[q.l];
-                            ok = ok && s_tab[(q.l * 5 + item_row(q.kind, q.sl)) * nmax + dl] != (T)0;
+                    if (qi.kind != QI_OWN) {
+                        const int dk = (tile / tsh[qi.k]) % snf[qi.k];
+                        ok = s_tab[(qi.k * 5 + item_row(qi.kind, qi.sk)) * nmax + dk] != (T)0;
+                        if (qi.kind == QI_PAIR) {
+                            const int dl = (tile / tsh[qi.l]) % snf[qi.l];
+                            ok = ok && s_tab[(qi.l * 5 + item_row(qi.kind, qi.sl)) * nmax + dl] != (T)0;
                         }
                     }
                 }
                 const unsigned bal = __ballot_sync(0xffffffffu, ok);
-                if (lane == w) myw = bal;
+                if (ok) pl[1 + base + __popc(bal & ((1u << lane) - 1u))] = it;
+                base += __popc(bal);
             }
-            const long long tb = (long long)tile * TF;
-            for (int w = 0; w < nw; ++w) {
-                unsigned bits = __shfl_sync(0xffffffffu, myw, w);
-                while (bits) {
-                    const int it = (w << 5) + __ffs(bits) - 1;
-                    bits &= bits - 1;
-                    if (lane == 0 && !stop) {
-                        const QuadItem q = s_it[it];
-                        if (mbar_wait(&empty[slot], ph ^ 1u, abort_flag, A.wait_limit)) {
-                            mbar_expect_tx(&full[slot], bytes);
-                            bulk_g2s(s_ring + slot * sst + pad, x + q.b * N + tb + (long long)q.tshift * TF, bytes,
-                                     &full[slot]);
-                            ++issued;
-                        } else {
-                            stop = 1;
-                        }
+            if (lane == 0) pl[0] = base;
+            __syncwarp();
+        };
+        int slot = 0;
+        unsigned ph = 0;
+        long long issued = 0;
+        int stop = A.nocopy;
+        if (blockIdx.x < A.ntiles) list(blockIdx.x, 0);
+        int q = 0;
+        for (int tile = blockIdx.x; tile < A.ntiles && !stop; tile += gridDim.x, q ^= 1) {
+            if (tile + (int)gridDim.x < A.ntiles) list(tile + gridDim.x, q ^ 1);
+            const int *pl = s_pl + q * (nit + 1);
+            const int cnt = pl[0];
+            if (lane == 0) {
+                const long long tb = (long long)tile * TF;
+                for (int i = 0; i < cnt && !stop; ++i) {
+                    const QuadItem qi = s_it[pl[1 + i]];
+                    if (mbar_wait(&empty[slot], ph ^ 1u, abort_flag, A.wait_limit)) {
+                        mbar_expect_tx(&full[slot], bytes);
+                        bulk_g2s(s_ring + slot * sst + pad, x + qi.b * N + tb + (long long)qi.tshift * TF, bytes,
+                                 &full[slot]);
+                        ++issued;
+                    } else {
+                        stop = 1;
                     }
                     if (++slot == NS) {
                         slot = 0;
@@ -540,7 +550,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                         }
                         const T c0 = rc[j * (NF + 1)], c1 = rc[(j + 1) * (NF + 1)];
 #pragma unroll
-                        for (int r = 0; r < R; ++r) acc[r] += c0 * v0[r] + c1 * v1[r];
+                        for (int r = 0; r < R; ++r) acc[r] = fma(c1, v1[r], fma(c0, v0[r], acc[r]));
                     }
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&empty[s0]);

@@ -96,7 +96,7 @@ struct QuadPlan {
 
 // Shared-memory layout (byte offsets), identical on host and device.
 struct QuadLayout {
-    int tab, G, R, Q, cst, om, sd, se, dt, items, cnt, rec, ring, z, total;
+    int tab, G, R, Q, cst, om, sd, se, dt, items, cnt, plist, rec, ring, z, total;
 };
 constexpr int QUAD_MAXSLOT = 16;
 __host__ __device__ inline QuadLayout quad_layout(int M, int S, int nmax, int m, int nF, int sstate, int eb,
@@ -119,6 +119,7 @@ __host__ __device__ inline QuadLayout quad_layout(int M, int S, int nmax, int m,
     L.dt = take(2 * (S * S + 1) * eb);
     L.items = take(nitems * (int)sizeof(QuadItem) + (3 * QUAD_MAXS + 1) * 4);
     L.cnt = take(2 * QUAD_MAXS * 2 * 4);            // per tile parity and target: Z items, slow items present
+    L.plist = take(2 * (nitems + 1) * 4);           // producer: per tile parity, count and present items
     L.rec = take(2 * nitems * (nF + 1) * eb);       // per tile parity: c, z[nF] of the present slow items
     o = (o + 127) / 128 * 128;
     L.ring = take(nslot * sstate * eb);
