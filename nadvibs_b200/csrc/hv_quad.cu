@@ -13,8 +13,9 @@
 //   slow +-1:     y_a += G^ab_k e x_b(p+-e_k), Z_l += Q^a_kl e x_a(p+-e_k);
 //   slow +-2:     y_a += R^ab_k e x_b(p+-2e_k);
 //   slow pairs:   y_a += Q^a_kl e x_a(p+-e_k+-e_l);
-// with e the tile's slow element factor.  Finally Z_l (l > m) goes to shared memory and
-// y_a += X_l Z_l (register shifts along m).  Out-of-basis neighbours have element factor 0
+// with e the tile's slow element factor.  Finally y_a += X_l Z_l: by register shifts for
+// l = m, and for each other fast mode through one shared-memory buffer (one mode at a time,
+// so that the buffer costs one ring slot, not NF - 1).  Out-of-basis neighbours have element factor 0
 // (the item is skipped by producer and consumers alike) and zero-filled halos.
 // Every wait is bounded: a wait that runs out raises a CTA abort flag, after which no thread
 // waits again and the kernel reports the failure through its error word.
@@ -131,7 +132,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
     T *s_rec = reinterpret_cast<T *>(smem + Lo.rec);      // [2][nitems][NF+1]
     int *s_ib = reinterpret_cast<int *>(smem + Lo.items + A.nitems * (int)sizeof(QuadItem));
     T *s_ring = reinterpret_cast<T *>(smem + Lo.ring);  // [NS][sst]
-    T *s_z = reinterpret_cast<T *>(smem + Lo.z);        // [NF-1][sst] Z_l, l > m
+    T *s_z = reinterpret_cast<T *>(smem + Lo.z);        // [sst] Z_l of one fast mode l > m
     const int tid = threadIdx.x;
     const int nc = NC > 0 ? NC : (int)blockDim.x - 32;  // consumer threads = shft(m)
     const long long N = A.dimen;
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
         }
         for (int i = tid; i < A.nitems; i += blockDim.x) s_it[i] = A.items[i];
         for (int i = tid; i <= 3 * S; i += blockDim.x) s_ib[i] = A.item_beg[i];
-        const int nz = (NS + (NF > 1 ? NF - 1 : 1)) * sst;  // ring and Z are contiguous
+        const int nz = (NS + 1) * sst;  // ring and Z are contiguous
         for (int i = tid; i < nz; i += blockDim.x) s_ring[i] = (T)0;
     }
     if (tid == 0) {
@@ -566,23 +567,26 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                     release();
                 }
             }
-            // y_a += X_l Z_l
-#pragma unroll
-            for (int j = 1; j < NF; ++j)
-#pragma unroll
-                for (int r = 0; r < R; ++r) s_z[(j - 1) * sst + pad + r * nc + tid] = r < nv ? Z[j][r] : (T)0;
-            consumer_sync(nc);
+            // y_a += X_l Z_l: mode m by register shifts, the other fast modes one at a time
+            // through a single shared-memory buffer
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 T v = acc[r];
                 if (r + 1 < R) v += F.em[0][r] * Z[0][r + 1];
                 if (r >= 1) v += F.em[1][r] * Z[0][r - 1];
-#pragma unroll
-                for (int j = 1; j < NF; ++j) {
-                    const T *p = s_z + (j - 1) * sst + pad + r * nc + tid;
-                    v += e1p[j] * p[F.sh[j]] + e1m[j] * p[-F.sh[j]];
-                }
                 acc[r] = v;
+            }
+#pragma unroll
+            for (int j = 1; j < NF; ++j) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) s_z[pad + r * nc + tid] = r < nv ? Z[j][r] : (T)0;
+                consumer_sync(nc);
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const T *p = s_z + pad + r * nc + tid;
+                    acc[r] += e1p[j] * p[F.sh[j]] + e1m[j] * p[-F.sh[j]];
+                }
+                consumer_sync(nc);  // s_z is rewritten next
             }
 #pragma unroll
             for (int r = 0; r < R; ++r)
@@ -591,7 +595,6 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                     y[a * N + tbase + r * nc + tid] = v;
                     if (alpha_part) part += ((double)xr[r] * (double)sc) * (double)v;
                 }
-            consumer_sync(nc);  // s_z is rewritten by the next state
         }
     }
     if (*abort_flag && tid == 0) atomicExch(A.err, 1);

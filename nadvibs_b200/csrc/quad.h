@@ -123,7 +123,7 @@ __host__ __device__ inline QuadLayout quad_layout(int M, int S, int nmax, int m,
     L.rec = take(2 * nitems * (nF + 1) * eb);       // per tile parity: c, z[nF] of the present slow items
     o = (o + 127) / 128 * 128;
     L.ring = take(nslot * sstate * eb);
-    L.z = take((nF > 1 ? nF - 1 : 1) * sstate * eb);
+    L.z = take(sstate * eb);
     L.total = o;
     return L;
 }
