@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient (grad/fwd) measurement")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the mixed-vs-FP64 Ritz comparison")
+    ap.add_argument("--config5", action="store_true",
+                    help="also run the large cubic system (config 5): literal-size mixed forward and the "
+                         "budgeted gradient (minutes; not part of the default run)")
     ap.add_argument("--basis", type=str, default=None,
                     help="comma-separated basis overriding the config's (same coefficients; profiling of "
                          "reduced sizes)")
@@ -294,6 +297,79 @@ def grad_timing(dev: int):
             "grad_over_fwd": g / f}
 
 
+def large_cubic(dev: int, iters: int = 4, warm: int = 2, grad_iters: int = 60, budget: float = 150e9):
+    """Config 5, ordr 3 (cubic terms N(0,10 cm^-1)), 3 states, 10 modes, FP32 vectors / FP64
+    recurrence.  (1) The literal basis [16,14,12,10,8,8,6,6,4,4]: 990,904,320 functions per
+    state, 2,972,712,960 elements, 11.9 GB per FP32 vector; `warm` + `iters` mixed iterations,
+    iter/s and the H.v kernel in use.  (2) The gradient at the size the benchmark description
+    states (~124M per state, 372M total): basis [8,7,6,10,8,8,6,6,4,4] with the same coefficient
+    draws; `grad_iters` mixed iterations, loss = Gaussian-convolved spectrum (sigma 20 cm^-1,
+    2048 points) + lowest 20 Ritz energies, reverse sweep with the automatic checkpoint plan
+    under a `budget`-byte device-memory budget.  Host wall times around synchronised calls."""
+    import numpy as np
+    import torch
+    from nadvibs_b200 import _lib as L
+    from nadvibs_b200 import synth
+    from nadvibs_b200.autograd import AU2WAVE, convolved_spectrum, tridiag_eig_backward, tridiag_eigh
+    cfg = synth.config(5)
+    om, cc, pot = synth.draw(cfg)
+    potf = synth.flatten_pot(pot)
+
+    def params(basis, niter):
+        p = L.default_params()
+        p.nstates, p.nmodes, p.ordr, p.niter = cfg.nstates, cfg.nmodes, cfg.ordr, niter
+        for i, b in enumerate(basis):
+            p.basis[i] = b
+        return p
+
+    out = {}
+    h = L.Handle.from_arrays(params(cfg.basis, warm + iters), om, cc, potf, device=dev, precision=L.NVB_MIXED)
+    try:
+        free, total = torch.cuda.mem_get_info(dev)
+        h.seed()
+        h.lanczos(warm)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h.lanczos(iters)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out["literal"] = {"basis": list(cfg.basis), "elements": int(np.prod(cfg.basis)) * cfg.nstates,
+                          "kernel": h.hv_kernel(L.DTYPE_F32), "iter_per_s": iters / dt, "ms_per_iter": 1e3 * dt / iters,
+                          "device_gb_in_use_after_create": (total - free) / 1e9, "iterations_timed": iters}
+    finally:
+        h.close()
+    basis = [8, 7, 6, 10, 8, 8, 6, 6, 4, 4]
+    n = grad_iters
+    h = L.Handle.from_arrays(params(basis, n), om, cc, potf, device=dev, precision=L.NVB_MIXED)
+    try:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h.seed()
+        a, b = h.lanczos(n)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        E, S = tridiag_eigh(a[:n], b[1:n])
+        grid = torch.linspace(-200.0, 8000.0, 2048, dtype=torch.float64)
+        w = torch.from_numpy(np.random.default_rng(5).normal(size=2048))
+        Et = torch.from_numpy(E).requires_grad_(True)
+        It = torch.from_numpy(S[0] ** 2).requires_grad_(True)
+        ((w * convolved_spectrum(Et, It, grid, 20.0)).sum() + (Et[:20] * AU2WAVE).sum()).backward()
+        abar, boff = tridiag_eig_backward(E, S, Et.grad.numpy(), It.grad.numpy())
+        bbar = np.zeros(n)
+        bbar[: n - 1] = boff
+        h.set_backward_memory(int(budget))
+        g = h.lanczos_backward(n, abar, bbar, 0)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        out["gradient"] = {"basis": basis, "elements": int(np.prod(basis)) * cfg.nstates, "iterations": n,
+                           "budget_gb": budget / 1e9, "backward_plan": h.backward_plan(), "ncoef": int(g.size),
+                           "finite": bool(np.isfinite(g).all()), "fwd_s": t1 - t0, "grad_s": t2 - t1,
+                           "grad_over_fwd": (t2 - t1) / (t1 - t0)}
+    finally:
+        h.close()
+    return out
+
+
 def cpu_baseline_sample(cfgn: int, iters: int):
     """The oracle's restatement of the reference (one streaming pass per term and shift,
     Source/top.f90:672-818, and lanczos_step) on all host cores, bounded sample."""
@@ -368,6 +444,8 @@ def main():
         line["fp64_hv_ms"] = r["hv_ms_per"]
     if rank == 0 and not args.no_grad:
         line["grad"] = grad_timing(local)
+    if rank == 0 and args.config5:
+        line["config5"] = large_cubic(local)
     if rank == 0 and "mixed" in res and not args.no_accuracy:
         tmp = tempfile.mkdtemp(prefix="nvb_acc_")
         _, (b_in, n_in) = make_inputs(args.config, tmp, args.basis)
