@@ -1,9 +1,11 @@
 // Slab-tiled H.v (see slab.h for the decomposition).  One CTA per tile of T_F rows (fixed
 // slow digits), SLAB_RPT rows per thread.
 //
-// Prologue: the CTA folds, for every step, the slow element factors of its tile (uniform over
-// the CTA) into the S x S coupling block of the step's term and packs the step's fast part
-// (shift, fast table rows, state masks) into shared memory.
+// Prologue: the CTA computes, for every step, the slow element factor of its tile (uniform
+// over the CTA) into shared memory; the step's packed fast part (shift, fast table rows,
+// state masks) and its term's S x S coupling block are tile-independent tables in global
+// memory, read through L1 (this keeps the CTA's shared memory small, so that several CTAs
+// share a multiprocessor on systems with thousands of steps).
 // Staged groups (steps with fast shifts, and the own tile): the neighbour tile x(p + sigma_S)
 // is copied to shared memory by TMA bulk copies (cp.async.bulk, one per source state) that
 // complete on an mbarrier; two buffers alternate so the copy of the next staged group
@@ -24,6 +26,8 @@ namespace nvb {
 template <typename T>
 struct SlabArgs {
     const SlabStep *steps;
+    const int4 *info;  // [nsteps] packed fast part of each step
+    const T *scoef;    // [nsteps][S][S] coupling block of each step's term
     int nsteps;
     const SlabGroup *groups;
     int ngroups;
@@ -108,9 +112,8 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
     T *s_ftab = reinterpret_cast<T *>(smem + Lo.ftab);
     T *s_etab = reinterpret_cast<T *>(smem + Lo.etab);
-    T *s_cm = reinterpret_cast<T *>(smem + Lo.cm);
+    T *s_sf = reinterpret_cast<T *>(smem + Lo.sf);  // [nsteps] slow element factor of each step
     T *s_cg = reinterpret_cast<T *>(smem + Lo.cg);
-    int4 *s_info = reinterpret_cast<int4 *>(smem + Lo.info);
     int *s_sd = reinterpret_cast<int *>(smem + Lo.sd);
     T *s_buf = reinterpret_cast<T *>(smem + Lo.buf);
     const int stride_state = (int)A.sstate;  // shared-memory offsets fit in 32 bits
@@ -139,39 +142,23 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
             for (int i = A.pad + TF + tid; i < stride_state; i += nth) base[i] = (T)0;
         }
     __syncthreads();
-    // per-CTA step tables
+    // per-CTA slow element factor of every step (zero where the slow neighbour leaves the
+    // basis); the step's fast part and coupling block are tile-independent (A.info, A.scoef)
     for (int i = tid; i < A.nsteps; i += nth) {
         const SlabStep *st = A.steps + i;
         T sf = 1;
-        bool ok = true;
         const int nsl = st->nslow;
         for (int q = 0; q < nsl; ++q) {
             const int md = st->slow_mode[q];
             const int n = s_sd[md];
             const int nc = n + st->slow_sig[q];
             if (nc < 0 || nc >= A.slow_nfunc[md]) {
-                ok = false;
+                sf = 0;
                 break;
             }
             sf = sf * s_etab[st->slow_etab[q] + (nc < n ? nc : n)];
         }
-        const int term = st->term;
-        const unsigned pm = ok ? (unsigned)(A.mask[2 * term] & 0xFFFFull) : 0u;
-        unsigned cols = 0;
-#pragma unroll
-        for (int ab = 0; ab < S2; ++ab) {
-            const bool on = (pm >> ab) & 1u;
-            s_cm[i * S2 + ab] = on ? A.coef[(size_t)term * S2 + ab] * sf : (T)0;
-            if (on) cols |= 1u << (ab % S);
-        }
-        const int nfa = st->nfast;
-        unsigned w = (unsigned)nfa | (cols << 11) | (pm << 15);
-        int fr[4] = {0, 0, 0, 0};
-        for (int q = 0; q < nfa; ++q) {
-            w |= (unsigned)st->fast_field[q] << (3 + 2 * q);
-            fr[q] = st->fast_row[q];
-        }
-        s_info[i] = make_int4(st->stride, (int)w, fr[0] | (fr[1] << 16), fr[2] | (fr[3] << 16));
+        s_sf[i] = sf;
     }
     __syncthreads();
     // direct groups: the sum of their steps' blocks (uniform over the tile)
@@ -180,9 +167,11 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
         T C[S2];
 #pragma unroll
         for (int ab = 0; ab < S2; ++ab) C[ab] = 0;
-        for (int i = G->step_begin; i < G->step_end; ++i)
+        for (int i = G->step_begin; i < G->step_end; ++i) {
+            const T sf = s_sf[i];
 #pragma unroll
-            for (int ab = 0; ab < S2; ++ab) C[ab] += s_cm[i * S2 + ab];
+            for (int ab = 0; ab < S2; ++ab) C[ab] += __ldg(A.scoef + (size_t)i * S2 + ab) * sf;
+        }
 #pragma unroll
         for (int ab = 0; ab < S2; ++ab) s_cg[(q - A.nstaged) * S2 + ab] = C[ab];
     }
@@ -345,7 +334,7 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
         }
         const int sbeg = A.groups[g].step_begin, send = A.groups[g].step_end;
         for (int i = sbeg; i < send; ++i) {
-            const int4 inf = s_info[i];
+            const int4 inf = __ldg(A.info + i);
             const unsigned w = (unsigned)inf.y;
             const int nfa = info_nfast(w);
             T e[SLAB_RPT];
@@ -389,7 +378,8 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
                 }
             }
             const unsigned cols = info_cols(w), pairs = info_pairs(w);
-            const T *cm = s_cm + i * S2;
+            const T sfi = s_sf[i];
+            const T *cm = A.scoef + (size_t)i * S2;
 #pragma unroll
             for (int b = 0; b < S; ++b) {
                 if (!((cols >> b) & 1u)) continue;
@@ -404,7 +394,7 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
 #pragma unroll
                 for (int a = 0; a < S; ++a)
                     if ((pairs >> (a * S + b)) & 1u) {
-                        const T c = cm[a * S + b];
+                        const T c = __ldg(cm + a * S + b) * sfi;
 #pragma unroll
                         for (int k = 0; k < SLAB_RPT; ++k) acc[a][k] = acc[a][k] + c * xb[k];
                     }
@@ -455,6 +445,7 @@ template <typename T>
 static SlabArgs<T> slab_args(const SlabPlan &sp, const Plan &pl) {
     SlabArgs<T> a{};
     a.steps = sp.d_steps;
+    a.info = sp.d_info;
     a.nsteps = (int)sp.steps.size();
     a.groups = sp.d_groups;
     a.ngroups = (int)sp.groups.size();
@@ -480,6 +471,7 @@ static SlabArgs<T> slab_args(const SlabPlan &sp, const Plan &pl) {
         a.ftab = (const T *)sp.d_ftab;
         a.etab = (const T *)pl.d_etab;
         a.coef = (const T *)pl.d_coef;
+        a.scoef = (const T *)sp.d_scoef;
         a.cst = (const T *)pl.d_const;
         a.slow_omega = (const T *)sp.d_slow_omega;
         a.fast_omega = (const T *)sp.d_fast_omega;
@@ -487,6 +479,7 @@ static SlabArgs<T> slab_args(const SlabPlan &sp, const Plan &pl) {
         a.ftab = (const T *)sp.d_ftab_f;
         a.etab = (const T *)pl.d_etab_f;
         a.coef = (const T *)pl.d_coef_f;
+        a.scoef = (const T *)sp.d_scoef_f;
         a.cst = (const T *)pl.d_const_f;
         a.slow_omega = (const T *)sp.d_slow_omega_f;
         a.fast_omega = (const T *)sp.d_fast_omega_f;

@@ -75,7 +75,15 @@ struct SlabPlan {
     std::vector<int> fast_nfunc;        // [nF]
     std::vector<long long> fast_shft;   // [nF]
     std::vector<double> fast_omega;     // [nF]
+    // per-step constants (the same for every tile), read through L1 by the kernel: packed fast
+    // part (stride, nfast | fields | column mask | pair mask, fast table rows) and the S x S
+    // coupling block of the step's term (zero outside its state pairs)
+    std::vector<int4> info;             // [nsteps]
+    std::vector<double> scoef;          // [nsteps][S][S]
     // device copies
+    int4 *d_info = nullptr;
+    double *d_scoef = nullptr;
+    float *d_scoef_f = nullptr;
     SlabStep *d_steps = nullptr;
     SlabGroup *d_groups = nullptr;
     SlabDiag *d_diag = nullptr;
@@ -95,7 +103,7 @@ struct SlabPlan {
 
 // Dynamic shared-memory layout of the slab kernel (byte offsets), shared by host and device.
 struct SlabLayout {
-    size_t ftab, etab, cm, cg, info, sd, buf, total;
+    size_t ftab, etab, sf, cg, sd, buf, total;
 };
 __host__ __device__ inline SlabLayout slab_layout(long long ftab_len, long long etab_len, long long nsteps,
                                                   long long ndirect, int S, int m, long long sstate, int eb) {
@@ -105,13 +113,11 @@ __host__ __device__ inline SlabLayout slab_layout(long long ftab_len, long long 
     off += (size_t)ftab_len * eb;
     L.etab = off;
     off += (size_t)etab_len * eb;
-    L.cm = off;
-    off += (size_t)nsteps * S * S * eb;
+    L.sf = off;
+    off += (size_t)nsteps * eb;
     L.cg = off;
     off += (size_t)ndirect * S * S * eb;
     off = (off + 15) / 16 * 16;
-    L.info = off;
-    off += (size_t)nsteps * 16;
     L.sd = off;
     off += (size_t)m * 4 + 16;
     off = (off + 127) / 128 * 128;

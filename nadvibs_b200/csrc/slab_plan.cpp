@@ -213,6 +213,27 @@ bool slab_build(SlabPlan &sp, const Plan &pl, const System &sys, int quirk_cubic
     sp.nfrows = (int)frow.size();
     if (sp.ftab.empty()) sp.ftab.assign(sp.frow_len, 0.0);
     if (sp.ftab.size() > 65535) return false;  // fast row offsets are packed in 16 bits
+    // per-step constants: word = nfast (3 bits) | fast fields (4 x 2 bits) << 3 | column mask
+    // (4) << 11 | pair mask (16) << 15, and the term's coupling block on its state pairs
+    sp.info.resize(sp.steps.size());
+    sp.scoef.assign(sp.steps.size() * (size_t)S * S, 0.0);
+    for (size_t i = 0; i < sp.steps.size(); ++i) {
+        const SlabStep &st = sp.steps[i];
+        const unsigned pm = (unsigned)(pl.h_mask[2 * (size_t)st.term] & 0xFFFFull);
+        unsigned cols = 0;
+        for (int ab = 0; ab < S * S; ++ab)
+            if ((pm >> ab) & 1u) {
+                cols |= 1u << (ab % S);
+                sp.scoef[i * S * S + ab] = pl.h_coef[(size_t)st.term * S * S + ab];
+            }
+        unsigned w = (unsigned)st.nfast | (cols << 11) | (pm << 15);
+        int fr[4] = {0, 0, 0, 0};
+        for (int q = 0; q < st.nfast; ++q) {
+            w |= (unsigned)st.fast_field[q] << (3 + 2 * q);
+            fr[q] = st.fast_row[q];
+        }
+        sp.info[i] = make_int4(st.stride, (int)w, fr[0] | (fr[1] << 16), fr[2] | (fr[3] << 16));
+    }
     sp.smem_bytes[0] = slab_smem(sp, pl, 8);
     sp.smem_bytes[1] = slab_smem(sp, pl, 4);
     if (sp.smem_bytes[eb == 8 ? 0 : 1] > 227 * 1024) return false;
@@ -248,6 +269,9 @@ void slab_upload(SlabPlan &sp) {
     up(sp.d_fast_shft, sp.fast_shft);
     up(sp.d_fast_omega, sp.fast_omega);
     up(sp.d_fast_omega_f, std::vector<float>(sp.fast_omega.begin(), sp.fast_omega.end()));
+    up(sp.d_info, sp.info);
+    up(sp.d_scoef, sp.scoef);
+    up(sp.d_scoef_f, std::vector<float>(sp.scoef.begin(), sp.scoef.end()));
     CK(cudaMalloc((void **)&sp.d_err, sizeof(int)));
     CK(cudaMemset(sp.d_err, 0, sizeof(int)));
 }
@@ -255,13 +279,14 @@ void slab_upload(SlabPlan &sp) {
 void slab_free(SlabPlan &sp) {
     void *ps[] = {sp.d_steps, sp.d_groups, sp.d_diag, sp.d_ftab, sp.d_ftab_f, sp.d_slow_tshft, sp.d_slow_nfunc,
                   sp.d_slow_omega, sp.d_slow_omega_f, sp.d_fast_nfunc, sp.d_fast_shft, sp.d_fast_omega,
-                  sp.d_fast_omega_f, sp.d_err};
+                  sp.d_fast_omega_f, sp.d_err, sp.d_info, sp.d_scoef, sp.d_scoef_f};
     for (void *p : ps)
         if (p) cudaFree(p);
     sp.d_steps = nullptr; sp.d_groups = nullptr; sp.d_diag = nullptr; sp.d_ftab = nullptr; sp.d_ftab_f = nullptr;
     sp.d_slow_tshft = nullptr; sp.d_slow_nfunc = nullptr; sp.d_slow_omega = nullptr; sp.d_slow_omega_f = nullptr;
     sp.d_fast_nfunc = nullptr; sp.d_fast_shft = nullptr; sp.d_fast_omega = nullptr; sp.d_fast_omega_f = nullptr;
     sp.d_err = nullptr;
+    sp.d_info = nullptr; sp.d_scoef = nullptr; sp.d_scoef_f = nullptr;
 }
 
 }  // namespace nvb
