@@ -324,33 +324,46 @@ static void launch_chunk(nvb_handle *h, const std::vector<AdjStep> &steps, const
     cudaFree(d);
 }
 
-// P[m][a][b] for the monomials of an ordr <= 2 system and Cq = (C[a][b], K_k), via the Gram matrix.
+// Length of the raw Gram output of the ordr <= 2 path: G1 = u^T B (S x nB), G2 = (X u)^T (X v)
+// (MS x MS), with A = [u (S), X u (M S)] and B = [v (S), X v (M S), x^2 v (M S), (n+1/2) v (M S)].
+static int gram_len(int S, int M) {
+    const int MS = M * S, nB = S + 3 * MS;
+    return S * nB + MS * MS;
+}
+
+static int gram_grid(const nvb_handle *h) {
+    return (int)std::min<long long>((h->sys.dimen + GRAM_TR - 1) / GRAM_TR, 148 * 4);
+}
+
+// G (+)= the Gram matrices of (u, v) on the device, through block partials part[gram_grid *
+// gram_len] (no host synchronisation).
 template <typename T>
-static void gram_adjoint(nvb_handle *h, const T *u, const T *v, const std::vector<Mono> &monos, std::vector<double> &P,
-                         std::vector<double> &Cq) {
+static void gram_launch(nvb_handle *h, const T *u, const T *v, double *G, int accumulate, double *part) {
     const System &sys = h->sys;
     const Plan &pl = h->plan;
     const int S = sys.S, M = sys.M;
-    // expanded columns: A = [u (S), X u (M S)], B = [v (S), X v (M S), x^2 v (M S), (n+1/2) v (M S)];
-    // two Grams: G1 = u^T B (S x nB), G2 = (X u)^T (X v) (MS x MS)
     const int MS = M * S, nA = S + MS, nB = S + 3 * MS;
-    const int n1 = S * nB, n2 = MS * MS, nout = n1 + n2;
+    const int nout = gram_len(S, M);
     if (!gram_fits(S, M)) fail(NVB_ERR_ARG, "adjoint: too many modes x states for the Gram path");
     const long long Ns = sys.dimen;
-    const int grid = (int)std::min<long long>((Ns + GRAM_TR - 1) / GRAM_TR, 148 * 4);
-    double *scr = (double *)scratch_vector(h, ((size_t)grid * nout + nout) * sizeof(double));
-    double *part = scr, *G = scr + (size_t)grid * nout;
+    const int grid = gram_grid(h);
     const size_t shm = (size_t)GRAM_TR * (nA + nB) * sizeof(double);
     if (shm > 48 * 1024) CK(cudaFuncSetAttribute(k_adj_gram<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     k_adj_gram<T><<<grid, 256, shm, h->stream>>>(u, v, pl.d_etab, pl.nmax, pl.d_nfunc, pl.d_shft, M, S, Ns, part);
-    k_gram_reduce<<<(nout + 255) / 256, 256, 0, h->stream>>>(part, grid, nout, 0, G);
+    k_gram_reduce<<<(nout + 255) / 256, 256, 0, h->stream>>>(part, grid, nout, accumulate, G);
     CK(cudaGetLastError());
-    std::vector<double> G1h(n1), G2h(n2);
-    CK(cudaMemcpyAsync(G1h.data(), G, n1 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(G2h.data(), G + n1, n2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    auto g = [&](int a, int j) { return G1h[(size_t)a * nB + j]; };            // <u_a, B_j>
-    auto g2 = [&](int k, int a, int l, int b) { return G2h[(size_t)(k * S + a) * MS + l * S + b]; };
+}
+
+// P[m][a][b] for the monomials of an ordr <= 2 system and Cq = (C[a][b], K_k) from the Gram
+// matrices (host copy Gh of length gram_len).
+static void gram_pc(const nvb_handle *h, const std::vector<double> &Gh, const std::vector<Mono> &monos,
+                    std::vector<double> &P, std::vector<double> &Cq) {
+    const System &sys = h->sys;
+    const int S = sys.S, M = sys.M;
+    const int MS = M * S, nB = S + 3 * MS;
+    const int n1 = S * nB;
+    auto g = [&](int a, int j) { return Gh[(size_t)a * nB + j]; };            // <u_a, B_j>
+    auto g2 = [&](int k, int a, int l, int b) { return Gh[n1 + (size_t)(k * S + a) * MS + l * S + b]; };
     const int nm = (int)monos.size();
     P.assign((size_t)nm * S * S, 0.0);
     for (int t = 0; t < nm; ++t) {
@@ -369,6 +382,76 @@ static void gram_adjoint(nvb_handle *h, const T *u, const T *v, const std::vecto
         for (int b = 0; b < S; ++b) Cq[a * S + b] = g(a, b);
     for (int k = 0; k < M; ++k)
         for (int a = 0; a < S; ++a) Cq[S * S + k] += g(a, S + 2 * M * S + k * S + a);
+}
+
+template <typename T>
+static void gram_adjoint(nvb_handle *h, const T *u, const T *v, const std::vector<Mono> &monos, std::vector<double> &P,
+                         std::vector<double> &Cq) {
+    const int nout = gram_len(h->sys.S, h->sys.M), grid = gram_grid(h);
+    double *part = (double *)scratch_vector(h, ((size_t)grid + 1) * nout * sizeof(double));
+    double *G = part + (size_t)grid * nout;
+    gram_launch<T>(h, u, v, G, 0, part);
+    std::vector<double> Gh(nout);
+    CK(cudaMemcpyAsync(Gh.data(), G, nout * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    gram_pc(h, Gh, monos, P, Cq);
+}
+
+// dL/dtheta in the layout of nvb_hv_adjoint_coeffs from P[m][a][b] = <u_a| monomial m |v_b> and
+// Cq = (C[a][b] = <u_a|v_b>, K_k = sum_a <u_a|(n_k+1/2)|v_a>); linear in (P, Cq).
+static void assemble_grad(const nvb_handle *h, const std::vector<Mono> &monos, const std::vector<double> &P,
+                          const std::vector<double> &Cq, double *grad) {
+    const System &sys = h->sys;
+    const int S = sys.S, M = sys.M;
+    const int nm = (int)monos.size();
+    const int nb = sys.nstblks();
+    const int64_t npot = (int64_t)sys.potterms.size();
+    std::vector<std::pair<int, int>> cp(nb);
+    for (int i = 1; i <= S; ++i)
+        for (int j = 1; j <= i; ++j) cp[i * (i - 1) / 2 + j - 1] = {i - 1, j - 1};
+    // monomial id of (order d, index k)
+    std::vector<int> mono_base(sys.ordr + 1, 0);
+    for (int d = 1; d <= sys.ordr; ++d) mono_base[d] = (d == 1 ? 0 : mono_base[d - 1] + (int)numut(M, d - 1));
+    std::vector<double> scale(nm, 1.0);
+    for (int t = 0; t < nm; ++t)
+        for (size_t l = 0; l < monos[t].modes.size(); ++l)
+            scale[t] /= std::sqrt(std::pow(sys.omega[monos[t].modes[l]], (double)monos[t].pows[l]));
+    for (int b = 0; b < nb; ++b) {
+        auto [i, j] = cp[b];
+        for (int d = 1; d <= sys.ordr; ++d) {
+            const int64_t off = sys.pot_offset[(size_t)b * sys.ordr + d - 1];
+            const int64_t cnt = numut(M, d);
+            for (int64_t k = 0; k < cnt; ++k) {
+                const int t = mono_base[d] + (int)k;
+                double g = P[(size_t)t * S * S + i * S + j];
+                if (i != j) g += P[(size_t)t * S * S + j * S + i];
+                grad[off + k] = scale[t] * g;
+            }
+        }
+        double gc = Cq[i * S + j];
+        if (i != j) gc += Cq[j * S + i];
+        grad[npot + b] = gc;
+    }
+    // frequencies: harmonic part plus the omega dependence of every scaled coefficient
+    for (int k = 0; k < M; ++k) grad[npot + nb + k] = Cq[S * S + k];
+    for (int b = 0; b < nb; ++b) {
+        auto [i, j] = cp[b];
+        for (int d = 1; d <= sys.ordr; ++d) {
+            const int64_t off = sys.pot_offset[(size_t)b * sys.ordr + d - 1];
+            const int64_t cnt = numut(M, d);
+            for (int64_t k = 0; k < cnt; ++k) {
+                const double c = sys.potterms[off + k];
+                if (c == 0.0) continue;
+                const int t = mono_base[d] + (int)k;
+                double g = P[(size_t)t * S * S + i * S + j];
+                if (i != j) g += P[(size_t)t * S * S + j * S + i];
+                for (size_t l = 0; l < monos[t].modes.size(); ++l) {
+                    const int md = monos[t].modes[l];
+                    grad[npot + nb + md] += -(double)monos[t].pows[l] / (2.0 * sys.omega[md]) * c * scale[t] * g;
+                }
+            }
+        }
+    }
 }
 
 template <typename T, int S>
@@ -444,55 +527,7 @@ static void adjoint_s(nvb_handle *h, const T *u, const T *v, double *grad) {
     for (int q = 0; q < nout; ++q)
         for (int g = 0; g < grid; ++g) Cq[q] += hq[(size_t)g * nout + q];
     }
-    // assemble
-    const int nb = sys.nstblks();
-    const int64_t npot = (int64_t)sys.potterms.size();
-    std::vector<std::pair<int, int>> cp(nb);
-    for (int i = 1; i <= S; ++i)
-        for (int j = 1; j <= i; ++j) cp[i * (i - 1) / 2 + j - 1] = {i - 1, j - 1};
-    // monomial id of (order d, index k)
-    std::vector<int> mono_base(sys.ordr + 1, 0);
-    for (int d = 1; d <= sys.ordr; ++d) mono_base[d] = (d == 1 ? 0 : mono_base[d - 1] + (int)numut(M, d - 1));
-    std::vector<double> scale(nm, 1.0);
-    for (int t = 0; t < nm; ++t)
-        for (size_t l = 0; l < monos[t].modes.size(); ++l)
-            scale[t] /= std::sqrt(std::pow(sys.omega[monos[t].modes[l]], (double)monos[t].pows[l]));
-    for (int b = 0; b < nb; ++b) {
-        auto [i, j] = cp[b];
-        for (int d = 1; d <= sys.ordr; ++d) {
-            const int64_t off = sys.pot_offset[(size_t)b * sys.ordr + d - 1];
-            const int64_t cnt = numut(M, d);
-            for (int64_t k = 0; k < cnt; ++k) {
-                const int t = mono_base[d] + (int)k;
-                double g = P[(size_t)t * S * S + i * S + j];
-                if (i != j) g += P[(size_t)t * S * S + j * S + i];
-                grad[off + k] = scale[t] * g;
-            }
-        }
-        double gc = Cq[i * S + j];
-        if (i != j) gc += Cq[j * S + i];
-        grad[npot + b] = gc;
-    }
-    // frequencies: harmonic part plus the omega dependence of every scaled coefficient
-    for (int k = 0; k < M; ++k) grad[npot + nb + k] = Cq[S * S + k];
-    for (int b = 0; b < nb; ++b) {
-        auto [i, j] = cp[b];
-        for (int d = 1; d <= sys.ordr; ++d) {
-            const int64_t off = sys.pot_offset[(size_t)b * sys.ordr + d - 1];
-            const int64_t cnt = numut(M, d);
-            for (int64_t k = 0; k < cnt; ++k) {
-                const double c = sys.potterms[off + k];
-                if (c == 0.0) continue;
-                const int t = mono_base[d] + (int)k;
-                double g = P[(size_t)t * S * S + i * S + j];
-                if (i != j) g += P[(size_t)t * S * S + j * S + i];
-                for (size_t l = 0; l < monos[t].modes.size(); ++l) {
-                    const int md = monos[t].modes[l];
-                    grad[npot + nb + md] += -(double)monos[t].pows[l] / (2.0 * sys.omega[md]) * c * scale[t] * g;
-                }
-            }
-        }
-    }
+    assemble_grad(h, monos, P, Cq, grad);
 }
 
 void hv_adjoint(nvb_handle *h, const void *u, const void *v, int dtype, double *grad) {
@@ -510,6 +545,31 @@ void hv_adjoint(nvb_handle *h, const void *u, const void *v, int dtype, double *
     default: fail(NVB_ERR_ARG, "the adjoint supports up to 4 states");
     }
 #undef ADJ_CASE
+}
+
+// Accumulated adjoint for the reverse sweep (ordr <= 2 systems whose Gram matrices fit): the
+// gradient is linear in the Gram matrices, so the sweep sums them on the device over all
+// steps and assembles the gradient once.
+int64_t adjoint_gram_len(const nvb_handle *h) {
+    return (h->sys.ordr <= 2 && gram_fits(h->sys.S, h->sys.M)) ? gram_len(h->sys.S, h->sys.M) : 0;
+}
+int64_t adjoint_gram_part_len(const nvb_handle *h) { return (int64_t)gram_grid(h) * adjoint_gram_len(h); }
+
+void adjoint_gram_add(nvb_handle *h, const void *u, const void *v, int dtype, double *G, int accumulate, double *part) {
+    if (dtype == NVB_DTYPE_F32) gram_launch<float>(h, (const float *)u, (const float *)v, G, accumulate, part);
+    else gram_launch<double>(h, (const double *)u, (const double *)v, G, accumulate, part);
+}
+
+void adjoint_gram_grad(nvb_handle *h, const double *G, double *grad) {
+    const int64_t nout = adjoint_gram_len(h);
+    if (nout == 0) fail(NVB_ERR_STATE, "adjoint: no Gram path for this system");
+    std::vector<double> Gh((size_t)nout);
+    CK(cudaMemcpyAsync(Gh.data(), G, nout * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const auto monos = all_monomials(h->sys);
+    std::vector<double> P, Cq;
+    gram_pc(h, Gh, monos, P, Cq);
+    assemble_grad(h, monos, P, Cq, grad);
 }
 
 int64_t ncoef_of(const nvb_handle *h) { return (int64_t)h->sys.potterms.size() + h->sys.nstblks() + h->sys.M; }

@@ -81,6 +81,35 @@ __global__ void k_replay(T *__restrict__ w, const T *__restrict__ c, const T *__
     }
 }
 
+// rbar = vb_next / beta_i + btot v_{i+1},  btot = bbar_i - <vb_next, v_{i+1}> / beta_i  (bbar_i and
+// the dot product read from device memory)
+__global__ void k_rbar(double *__restrict__ rbar, const double *__restrict__ vbn, const double *__restrict__ vn,
+                       double inv_be, const double *__restrict__ bbar_i, const double *__restrict__ dot1, long long n) {
+    const double btot = *bbar_i - *dot1 * inv_be;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        rbar[i] = inv_be * vbn[i] + btot * vn[i];
+}
+
+// atot = abar_i - <rbar, v_i>;  vb_cur += -alpha_i rbar + atot w_i;  wbar = rbar + atot v_i;
+// vb_prev += -beta_{i-1} rbar (when i > 1)
+__global__ void k_step(double *__restrict__ vbc, double *__restrict__ wbar, double *__restrict__ vbp,
+                       const double *__restrict__ rbar, const double *__restrict__ w, const double *__restrict__ vi,
+                       double al, double abar_i, const double *__restrict__ dot2, double bprev, int has_prev,
+                       long long n) {
+    const double atot = abar_i - *dot2;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double r = rbar[i];
+        vbc[i] = vbc[i] + (-al * r + atot * w[i]);
+        wbar[i] = 1.0 * r + atot * vi[i];
+        if (has_prev) vbp[i] = vbp[i] + (-bprev * r);
+    }
+}
+
+// bbar_{i-1} -= <rbar, v_{i-1}>
+__global__ void k_bbar_sub(double *__restrict__ bbar, const double *__restrict__ dot3) { *bbar -= *dot3; }
+
 struct DevBuf {
     void *p = nullptr;
     DevBuf() = default;
@@ -218,7 +247,6 @@ struct Sweep {
     int dt = NVB_DTYPE_F64, g = 1;
     int64_t n = 0, B = 2, bmax = 1;  // branching of a level, longest range reversed from storage
     void *b3[3] = {nullptr, nullptr, nullptr};
-    double *dsc = nullptr;
     void *segv = nullptr, *segw = nullptr;  // native v_{c-1}..v_{e+1} and w_c..w_e of a base range
     std::vector<double> segs;                // their scales
     double *vb_next = nullptr, *vb_cur = nullptr, *vb_prev = nullptr, *rbar = nullptr, *wbar = nullptr,
@@ -226,6 +254,11 @@ struct Sweep {
     std::vector<double> abar, bbar, gstep;
     double *grad = nullptr;
     int64_t nc = 0, replayed = 0;  // H.v applications of the replays
+    // device-side scalars of the reverse step (no host synchronisation inside a step): bbar,
+    // the step's three dot products, the replay's scales; the accumulated adjoint Gram
+    // matrices when the system has the Gram path (else the per-step host adjoint)
+    double *d_bbar = nullptr, *d_dots = nullptr, *d_rscal = nullptr, *G = nullptr, *gpart = nullptr;
+    bool gram_started = false;
 
     void to64(double *dst, const void *src, double sc) {
         if (mixed) k_to_f64<float><<<g, 256, 0, h->stream>>>(dst, (const float *)src, sc, N);
@@ -237,6 +270,12 @@ struct Sweep {
     // on_w(j, w) with w = H v_j (native) for j < last.
     template <typename FV, typename FW>
     void replay(const CkPair &P, int64_t c, int64_t last, FV on_v, FW on_w) {
+        // the scale of the current vector at each step, uploaded once
+        std::vector<double> scal((size_t)(last - c + 1));
+        scal[0] = P.scur;
+        for (int64_t j = c + 1; j <= last; ++j) scal[(size_t)(j - c)] = 1.0 / h->beta[j - 1];
+        // stream-ordered: the previous replay's H.v launches read the old scales first
+        CK(cudaMemcpyAsync(d_rscal, scal.data(), scal.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         CK(cudaMemcpyAsync(b3[0], P.prev, per, cudaMemcpyDeviceToDevice, h->stream));
         CK(cudaMemcpyAsync(b3[1], P.cur, per, cudaMemcpyDeviceToDevice, h->stream));
         int prev = 0, cur = 1, work = 2;
@@ -244,8 +283,7 @@ struct Sweep {
         for (int64_t j = c; j <= last; ++j) {
             on_v(j, b3[prev], sprev, b3[cur], scur);
             if (j == last) break;
-            CK(cudaMemcpyAsync(dsc, &scur, sizeof(double), cudaMemcpyHostToDevice, h->stream));
-            hv_any(h, b3[cur], b3[work], dt, dsc, nullptr, nullptr);
+            hv_any(h, b3[cur], b3[work], dt, d_rscal + (j - c), nullptr, nullptr);
             ++replayed;
             on_w(j, b3[work]);
             if (mixed)
@@ -257,7 +295,6 @@ struct Sweep {
                                                            (const double *)b3[prev], scur, sprev, h->alpha[j],
                                                            h->beta[j - 1], N);
             CK(cudaGetLastError());
-            CK(cudaStreamSynchronize(h->stream));  // dsc is rewritten next step
             const int op = prev;
             prev = cur;
             cur = work;
@@ -265,10 +302,7 @@ struct Sweep {
             sprev = scur;
             scur = 1.0 / h->beta[j];
         }
-        CK(cudaStreamSynchronize(h->stream));
     }
-
-    double dot(const double *a, const double *b) { return device_dot(h, a, 1.0, b, 1.0, NVB_DTYPE_F64); }
 
     // reverse steps e..c of a range whose v_{c-1}..v_{e+1} and w_c..w_e are in segv/segw
     void reverse_steps(int64_t c, int64_t e) {
@@ -280,18 +314,25 @@ struct Sweep {
             V(i, vi);
             if (i > 1) V(i - 1, vp);
             to64(w64, nat(segw, i - c), 1.0);  // w_i = H v_i from the replay
-            const double btot = bbar[i] - dot(vb_next, vn) / be;
-            k_lin<<<g, 256, 0, h->stream>>>(rbar, 1.0 / be, vb_next, btot, vn, 0, N);
-            const double atot = abar[i - 1] - dot(rbar, vi);
-            if (i > 1) bbar[i - 1] -= dot(rbar, vp);
-            k_lin<<<g, 256, 0, h->stream>>>(vb_cur, -al, rbar, atot, w64, 1, N);
-            k_lin<<<g, 256, 0, h->stream>>>(wbar, 1.0, rbar, atot, vi, 0, N);
-            if (i > 1) k_lin<<<g, 256, 0, h->stream>>>(vb_prev, -bprev, rbar, 0.0, nullptr, 1, N);
+            device_dot_async(h, vb_next, 1.0, vn, 1.0, NVB_DTYPE_F64, d_dots);
+            k_rbar<<<g, 256, 0, h->stream>>>(rbar, vb_next, vn, 1.0 / be, d_bbar + i, d_dots, N);
+            device_dot_async(h, rbar, 1.0, vi, 1.0, NVB_DTYPE_F64, d_dots + 1);
+            if (i > 1) {
+                device_dot_async(h, rbar, 1.0, vp, 1.0, NVB_DTYPE_F64, d_dots + 2);
+                k_bbar_sub<<<1, 1, 0, h->stream>>>(d_bbar + i - 1, d_dots + 2);
+            }
+            k_step<<<g, 256, 0, h->stream>>>(vb_cur, wbar, vb_prev, rbar, w64, vi, al, abar[i - 1], d_dots + 1, bprev,
+                                             i > 1 ? 1 : 0, N);
             hv_any(h, wbar, wv, NVB_DTYPE_F64, nullptr, nullptr, nullptr);  // H wbar
             k_lin<<<g, 256, 0, h->stream>>>(vb_cur, 1.0, wv, 0.0, nullptr, 1, N);
             CK(cudaGetLastError());
-            hv_adjoint(h, wbar, vi, NVB_DTYPE_F64, gstep.data());
-            for (int64_t q = 0; q < nc; ++q) grad[q] += gstep[q];
+            if (G) {
+                adjoint_gram_add(h, wbar, vi, NVB_DTYPE_F64, G, gram_started ? 1 : 0, gpart);
+                gram_started = true;
+            } else {
+                hv_adjoint(h, wbar, vi, NVB_DTYPE_F64, gstep.data());
+                for (int64_t q = 0; q < nc; ++q) grad[q] += gstep[q];
+            }
             // rotate: vbar_{i+1} <- vbar_i, vbar_i <- vbar_{i-1}, vbar_{i-1} <- 0
             double *t = vb_next;
             vb_next = vb_cur;
@@ -422,8 +463,7 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
     h->bw_plan[1] = W.B;
     h->bw_plan[2] = W.bmax;
     // base storage and work vectors
-    DevBuf segv((size_t)(W.bmax + 2) * W.per), segw((size_t)(W.bmax + 1) * W.per), b0(W.per), b1(W.per), b2(W.per),
-        dscb(sizeof(double));
+    DevBuf segv((size_t)(W.bmax + 2) * W.per), segw((size_t)(W.bmax + 1) * W.per), b0(W.per), b1(W.per), b2(W.per);
     DevBuf vbn(W.per64), vbc(W.per64), vbp(W.per64), rb(W.per64), wb(W.per64), wvb(W.per64), c0(W.per64),
         c1(W.per64), c2(W.per64), cw(W.per64);
     W.segv = segv.p;
@@ -432,7 +472,6 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
     W.b3[0] = b0.p;
     W.b3[1] = b1.p;
     W.b3[2] = b2.p;
-    W.dsc = (double *)dscb.p;
     W.vb_next = (double *)vbn.p;
     W.vb_cur = (double *)vbc.p;
     W.vb_prev = (double *)vbp.p;
@@ -449,6 +488,16 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
     W.abar.assign(abar_in, abar_in + n);
     W.bbar.assign(n + 1, 0.0);  // bbar[i] for beta_i, i = 0..n
     for (int64_t i = 1; i <= n; ++i) W.bbar[i] = bbar_in ? bbar_in[i - 1] : 0.0;
+    const int64_t glen = adjoint_gram_len(h), gplen = adjoint_gram_part_len(h);
+    DevBuf dscal((size_t)(2 * (n + 1) + 3) * sizeof(double)), gbuf((size_t)std::max<int64_t>(1, glen + gplen) * sizeof(double));
+    W.d_bbar = (double *)dscal.p;
+    W.d_rscal = W.d_bbar + (n + 1);
+    W.d_dots = W.d_rscal + (n + 1);
+    CK(cudaMemcpyAsync(W.d_bbar, W.bbar.data(), (n + 1) * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (glen > 0) {
+        W.G = (double *)gbuf.p;
+        W.gpart = W.G + glen;
+    }
     W.grad = grad;
     std::fill(grad, grad + W.nc, 0.0);
     W.gstep.assign(W.nc, 0.0);
@@ -468,6 +517,7 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
             W.reverse_range(P, 1 + s2 * top, std::min((s2 + 1) * top, n));
         }
     }
+    if (W.G) adjoint_gram_grad(h, W.G, grad);  // the gradient of the summed Gram matrices
     CK(cudaStreamSynchronize(h->stream));
     h->bw_plan[3] = W.replayed;
     check_kernel_flags(h);

@@ -78,6 +78,9 @@ void hv_any(nvb_handle *h, const void *x, void *y, int dtype, const double *scal
 void ensure_partials(nvb_handle *h, int64_t n);
 void check_kernel_flags(nvb_handle *h);
 double device_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, int dtype);
+// the same inner product (same kernels, same summation order) written to device memory, no
+// host synchronisation
+void device_dot_async(nvb_handle *h, const void *a, double sa, const void *b, double sb, int dtype, double *out_dev);
 void *scratch_vector(nvb_handle *h, size_t bytes);
 void grow_scalars_public(nvb_handle *h, int64_t need);
 void archive_ensure(nvb_handle *h, int64_t need);
@@ -85,6 +88,12 @@ void archive_push(nvb_handle *h, int64_t it);
 void save_restart(nvb_handle *h, const char *dir, const char *vdir);
 void load_restart(nvb_handle *h, const char *dir, const char *vdir);
 void hv_adjoint(nvb_handle *h, const void *u, const void *v, int dtype, double *grad);
+// reverse-sweep adjoint: Gram matrices accumulated on the device (length adjoint_gram_len, 0
+// when the system has no Gram path), partials buffer of adjoint_gram_part_len doubles
+int64_t adjoint_gram_len(const nvb_handle *h);
+int64_t adjoint_gram_part_len(const nvb_handle *h);
+void adjoint_gram_add(nvb_handle *h, const void *u, const void *v, int dtype, double *G, int accumulate, double *part);
+void adjoint_gram_grad(nvb_handle *h, const double *G, double *grad);
 void hellmann_feynman(nvb_handle *h, int64_t nroots, double *grad, double *energies);
 void displaced_seed(nvb_handle *h);
 double seed_fill(nvb_handle *h, void *buf, const std::vector<double> &w);

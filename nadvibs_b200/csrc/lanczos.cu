@@ -483,6 +483,18 @@ void lanczos_run(nvb_handle *h, int64_t niter) {
     }
 }
 
+void device_dot_async(nvb_handle *h, const void *a, double sa, const void *b, double sb, int dtype, double *out_dev) {
+    const long long n = h->ntotal();
+    const int g = grid_for(n);
+    ensure_partials(h, g + 1);
+    if (dtype == NVB_DTYPE_F32)
+        k_dot<float><<<g, RED_THREADS, 0, h->stream>>>((const float *)a, (const float *)b, sa, sb, n, h->d_part);
+    else
+        k_dot<double><<<g, RED_THREADS, 0, h->stream>>>((const double *)a, (const double *)b, sa, sb, n, h->d_part);
+    k_finalize<<<1, FIN_THREADS, 0, h->stream>>>(h->d_part, g, out_dev, 0, nullptr, nullptr, 0);
+    CK(cudaGetLastError());
+}
+
 double device_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, int dtype) {
     const long long n = h->ntotal();
     const int g = grid_for(n);
