@@ -175,7 +175,8 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_diag(const long long *__res
 // tile of rows into shared memory and accumulates both; block partials are summed in a fixed
 // order.
 
-constexpr int GRAM_TR = 64;      // rows per shared-memory tile
+constexpr int GRAM_TR = 64;      // rows per shared-memory tile (a multiple of 4)
+static_assert(GRAM_TR % 4 == 0, "the Gram sums are unrolled by 4 rows");
 constexpr int GRAM_MAXPER = 8;   // Gram outputs per thread: S*(3M+1)*S + (MS)^2 <= 8*256
 
 // Per block: for each tile of GRAM_TR rows, the expanded columns of those rows go to shared
@@ -194,6 +195,7 @@ __global__ void __launch_bounds__(256) k_adj_gram(const T *__restrict__ u, const
     const double *E2 = etab + (1 * ETAB_J + 2) * nmax;  // <m|x^2|m+2>
     const double *D2 = etab + (1 * ETAB_J + 0) * nmax;  // <m|x^2|m>
     const int tid = threadIdx.x, nth = blockDim.x;
+    const bool small = dimen <= 0xFFFFFFFFll;
     double acc[GRAM_MAXPER];
 #pragma unroll
     for (int q = 0; q < GRAM_MAXPER; ++q) acc[q] = 0.0;
@@ -218,7 +220,8 @@ __global__ void __launch_bounds__(256) k_adj_gram(const T *__restrict__ u, const
             long long rem = r;
             for (int k = 0; k < M; ++k) {
                 const long long sh = shft[k];
-                const int d = (int)(rem / sh);
+                // digit of mode k (32-bit division when the state block has < 2^32 rows)
+                const int d = small ? (int)((unsigned)rem / (unsigned)sh) : (int)(rem / sh);
                 rem -= (long long)d * sh;
                 const int nf = nfunc[k];
                 double xu = 0.0, xv = 0.0, tv = D2[d] * v0;
@@ -254,9 +257,16 @@ __global__ void __launch_bounds__(256) k_adj_gram(const T *__restrict__ u, const
                     ia = S + o2 / MS;
                     jb = S + (o2 - (o2 / MS) * MS);
                 }
-                double x = acc[q];
-                for (int r = 0; r < GRAM_TR; ++r) x += sA[r * nA + ia] * sB[r * nB + jb];
-                acc[q] = x;
+                // four independent partial sums: the FMA chain of one output is the latency
+                double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
+#pragma unroll 4
+                for (int r = 0; r < GRAM_TR; r += 4) {
+                    x0 += sA[r * nA + ia] * sB[r * nB + jb];
+                    x1 += sA[(r + 1) * nA + ia] * sB[(r + 1) * nB + jb];
+                    x2 += sA[(r + 2) * nA + ia] * sB[(r + 2) * nB + jb];
+                    x3 += sA[(r + 3) * nA + ia] * sB[(r + 3) * nB + jb];
+                }
+                acc[q] += (x0 + x1) + (x2 + x3);
             }
         }
         __syncthreads();
