@@ -246,7 +246,8 @@ def mixed_accuracy(basis: str, nadvibs: str, dev: int, iters: int = 300):
 def grad_timing(dev: int):
     """grad/fwd on the gradient system (config 4): forward = seed + 400 plain Lanczos
     iterations; backward = eigen-derivatives of T_400 for a loss (Gaussian-convolved spectrum,
-    sigma 20 cm^-1, 2048 points, plus the lowest 20 Ritz energies) and the reverse sweep
+    sigma 20 cm^-1, 2048 points, plus the lowest 20 Ritz energies; loss and eigen-derivative
+    products on the GPU, the tridiagonal eigensolve on the host) and the reverse sweep
     (nvb_lanczos_backward with the automatic checkpoint plan, k = 0).  Host wall times around
     synchronised calls, best of 3."""
     import numpy as np
@@ -262,8 +263,10 @@ def grad_timing(dev: int):
     for i, b in enumerate(cfg.basis):
         p.basis[i] = b
     n, k = 400, 0
-    grid = torch.linspace(-200.0, 8000.0, 2048, dtype=torch.float64)
-    w = torch.from_numpy(np.random.default_rng(4).normal(size=2048))
+    cuda = torch.device("cuda", dev)
+    # the loss and the eigen-derivatives of T_n run on the same GPU (FP64)
+    grid = torch.linspace(-200.0, 8000.0, 2048, dtype=torch.float64, device=cuda)
+    w = torch.from_numpy(np.random.default_rng(4).normal(size=2048)).to(cuda)
     fwd, bwd, sweep, host = [], [], [], []
     plan = None
     for _ in range(3):
@@ -275,10 +278,10 @@ def grad_timing(dev: int):
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         E, S = tridiag_eigh(a[:n], b[1:n])
-        Et = torch.from_numpy(E).requires_grad_(True)
-        It = torch.from_numpy(S[0] ** 2).requires_grad_(True)
+        Et = torch.from_numpy(E).to(cuda).requires_grad_(True)
+        It = torch.from_numpy(S[0] ** 2).to(cuda).requires_grad_(True)
         ((w * convolved_spectrum(Et, It, grid, 20.0)).sum() + (Et[:20] * AU2WAVE).sum()).backward()
-        abar, boff = tridiag_eig_backward(E, S, Et.grad.numpy(), It.grad.numpy())
+        abar, boff = tridiag_eig_backward(E, S, Et.grad.cpu().numpy(), It.grad.cpu().numpy(), device=cuda)
         bbar = np.zeros(n)
         bbar[: n - 1] = boff
         th = time.perf_counter()

@@ -49,8 +49,12 @@ def tridiag_eigh(alpha: np.ndarray, beta_off: np.ndarray):
 
 
 def tridiag_eig_backward(E: np.ndarray, S: np.ndarray, gE: np.ndarray | None, gI: np.ndarray | None,
-                         eps_rel: float = 1e-10):
-    """dL/dalpha (n) and dL/dbeta_1..n-1 (n-1) from dL/dE and dL/dI, I_i = S[0, i]^2."""
+                         eps_rel: float = 1e-10, device=None):
+    """dL/dalpha (n) and dL/dbeta_1..n-1 (n-1) from dL/dE and dL/dI, I_i = S[0, i]^2.
+
+    Only the diagonal and the first off-diagonal of Tbar = S M S^T are formed (one n^3 product,
+    S M, then row-wise dot products with S).  With `device` a CUDA device the product runs there
+    in FP64 (torch); the results come back as numpy arrays either way."""
     n = E.size
     inner = np.zeros((n, n))
     if gE is not None:
@@ -63,10 +67,18 @@ def tridiag_eig_backward(E: np.ndarray, S: np.ndarray, gE: np.ndarray | None, gI
         F = d / (d * d + eps * eps)
         np.fill_diagonal(F, 0.0)
         inner += F * ssb
-    Tb = S @ inner @ S.T
-    Tb = 0.5 * (Tb + Tb.T)
-    abar = np.diag(Tb).copy()
-    bbar = 2.0 * np.diag(Tb, 1)
+    if device is not None and torch.device(device).type == "cuda":
+        St = torch.from_numpy(np.ascontiguousarray(S)).to(device)
+        SM = St @ torch.from_numpy(inner).to(device)
+        diag = (SM * St).sum(dim=1)
+        up = (SM[:-1] * St[1:]).sum(dim=1)             # Tbar[i, i+1]
+        lo = (SM[1:] * St[:-1]).sum(dim=1)             # Tbar[i+1, i]
+        abar = diag.cpu().numpy()
+        bbar = (up + lo).cpu().numpy()                 # 2 * symmetrised off-diagonal
+        return abar, bbar
+    SM = S @ inner
+    abar = np.einsum("ij,ij->i", SM, S)
+    bbar = np.einsum("ij,ij->i", SM[:-1], S[1:]) + np.einsum("ij,ij->i", SM[1:], S[:-1])
     return abar, bbar
 
 
@@ -97,7 +109,8 @@ class LanczosRitz(torch.autograd.Function):
     def backward(ctx, gE, gI):
         gEn = None if gE is None else gE.detach().to("cpu", torch.float64).numpy()
         gIn = None if gI is None else gI.detach().to("cpu", torch.float64).numpy()
-        abar, bbar_off = tridiag_eig_backward(ctx.E, ctx.S, gEn, gIn)
+        dev = ctx.dev if torch.device(ctx.dev).type == "cuda" else None
+        abar, bbar_off = tridiag_eig_backward(ctx.E, ctx.S, gEn, gIn, device=dev)
         n = ctx.niter
         bbar = np.zeros(n)
         bbar[: n - 1] = bbar_off  # beta_n does not enter T_n

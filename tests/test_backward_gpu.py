@@ -81,6 +81,42 @@ def test_backward_matches_finite_differences(seed, nstates, basis, n):
     assert np.abs(g[idx] - fd).max() <= 2e-6 * scale, (g[idx], fd)
 
 
+def test_cubic_system_gradient_matches_finite_differences():
+    """ordr 3: the reverse sweep takes the per-coefficient adjoint (no Gram path) at every step;
+    central differences of the GPU forward, and the automatic plan against one level."""
+    p, theta = _system(81, 2, [4, 3, 3], ordr=3)
+    n = 10
+    rng = np.random.default_rng(81)
+    gE, gI = rng.normal(size=n), rng.normal(size=n)
+    g = _gradient(p, theta, n, gE, gI, k=0, record=False, quirk_lower=0)
+    g1 = _gradient(p, theta, n, gE, gI, k=3, record=False, quirk_lower=0)
+    assert np.abs(g - g1).max() <= 1e-12 * np.abs(g1).max()
+
+    def f(th):
+        E, I = _forward(p, th, n, quirk_lower=0)
+        return float(gE @ E + gI @ I)
+
+    idx = sorted(set(rng.choice(theta.size, size=min(14, theta.size), replace=False).tolist()) | {theta.size - 1})
+    # the cubic coefficients are small, so the relative step is tiny and the differences carry
+    # rounding noise: estimate it from two step sizes and allow the gradient that much beyond
+    # the 2e-6 bound of the quadratic tests
+    fd = _fd(f, theta, idx)
+    fd2 = _fd(f, theta, idx, rel=3e-5)
+    tol = 2e-6 * np.abs(fd).max() + 3.0 * np.abs(fd - fd2)
+    assert (np.abs(g[idx] - fd) <= tol).all(), (g[idx], fd, fd2)
+
+
+def test_eig_backward_on_the_gpu_matches_the_host():
+    rng = np.random.default_rng(82)
+    n = 60
+    E, S = tridiag_eigh(rng.normal(size=n), rng.uniform(0.2, 1.0, size=n - 1))
+    gE, gI = rng.normal(size=n), rng.normal(size=n)
+    a0, b0 = tridiag_eig_backward(E, S, gE, gI)
+    a1, b1 = tridiag_eig_backward(E, S, gE, gI, device="cuda:0")
+    scale = max(np.abs(a0).max(), np.abs(b0).max())
+    assert np.abs(a1 - a0).max() <= 1e-12 * scale and np.abs(b1 - b0).max() <= 1e-12 * scale
+
+
 def test_checkpoint_interval_and_recording_do_not_change_the_gradient():
     p, theta = _system(74, 2, [4, 3, 3])
     n = 13
