@@ -377,6 +377,34 @@ def large_cubic(dev: int, iters: int = 4, warm: int = 2, grad_iters: int = 60, b
     return out
 
 
+def hv_flops(cfg) -> float:
+    """Reference-equivalent arithmetic of one H.v, from the term table (the reference's pass
+    structure, Source/top.f90:717-806): 2 flops per row for every nonzero (monomial, nonzero
+    shift, ordered state pair) and for every diagonal-section term (one fused harmonic energy +
+    constant per state, plus the zero shift of each all-even monomial).  Rows where a shift
+    leaves the basis are counted too, so this is an upper bound of the reference's work."""
+    import math
+    from nadvibs_b200 import synth
+    _, _, pot = synth.draw(cfg)
+    S, M = cfg.nstates, cfg.nmodes
+    dimen = math.prod(cfg.basis)
+    shift_terms, diag_terms = 0, S
+    k = 0
+    for i in range(1, S + 1):
+        for j in range(1, i + 1):
+            mult = 1 if i == j else 2
+            for d in range(1, cfg.ordr + 1):
+                for t, mono in enumerate(synth.monomials(M, d)):
+                    if pot[k][d - 1][t] == 0.0:
+                        continue
+                    pows = [mono.count(q) for q in set(mono)]
+                    even = all(p % 2 == 0 for p in pows)
+                    shift_terms += mult * (math.prod(p + 1 for p in pows) - (1 if even else 0))
+                    diag_terms += mult if even else 0
+            k += 1
+    return 2.0 * dimen * (shift_terms + diag_terms)
+
+
 def cpu_baseline_sample(cfgn: int, iters: int):
     """The oracle's restatement of the reference (one streaming pass per term and shift,
     Source/top.f90:672-818, and lanczos_step) on all host cores, bounded sample."""
@@ -449,6 +477,14 @@ def main():
                          "hv_frac": m["bytes_hv"] / (m["hv_ms_per"] / 1e3) / 1e9 / peak,
                          "hv_traffic": traffic_for("hv_" + m["kernel"], "mixed"), "kernel": f"k_hv_{m['kernel']}"}
         line["fp64_hv_ms"] = r["hv_ms_per"]
+    if rank == 0:
+        # the arithmetic side of the roofline, reference-equivalent flops (the factorised
+        # kernels execute fewer; see hv_flops)
+        fl = hv_flops(cfg)
+        line["alu"] = {"algorithmic_gflop_per_hv": fl / 1e9,
+                       "achieved_tflops": fl / (r["hv_ms_per"] / 1e3) / 1e12, "precision": main_prec}
+        if "mixed" in res and main_prec != "mixed":
+            line["alu"]["mixed_achieved_tflops"] = fl / (res["mixed"]["hv_ms_per"] / 1e3) / 1e12
     if rank == 0 and not args.no_grad:
         line["grad"] = grad_timing(local)
     if rank == 0 and args.config5:
