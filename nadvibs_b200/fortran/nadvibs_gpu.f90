@@ -90,5 +90,31 @@ module nadvibs_gpu
       real(c_double), dimension(*), intent(out) :: energy_ev, amp, overlap
       character(kind=c_char), dimension(*), intent(in) :: sodata
     end function
+    ! gradient path (no reference counterpart): checkpoints of the forward, the reverse
+    ! sweep through the recurrence (k = 0: automatic plan within the memory budget), its
+    ! budget and the plan it used
+    integer(c_int) function nvb_set_checkpoints(h, k) bind(C, name="nvb_set_checkpoints")
+      import :: c_int, c_int64_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: k
+    end function
+    integer(c_int) function nvb_lanczos_backward(h, n, alpha_bar, beta_bar, k, grad) &
+        bind(C, name="nvb_lanczos_backward")
+      import :: c_int, c_int64_t, c_double, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: n, k
+      real(c_double), dimension(*), intent(in) :: alpha_bar, beta_bar
+      real(c_double), dimension(*), intent(out) :: grad
+    end function
+    integer(c_int) function nvb_set_backward_memory(h, nbytes) bind(C, name="nvb_set_backward_memory")
+      import :: c_int, c_int64_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: nbytes
+    end function
+    integer(c_int) function nvb_backward_plan(h, plan) bind(C, name="nvb_backward_plan")
+      import :: c_int, c_int64_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), dimension(4), intent(out) :: plan
+    end function
   end interface
 end module nadvibs_gpu
