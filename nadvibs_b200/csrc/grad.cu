@@ -25,6 +25,12 @@
 // k = 0 the shallowest depth L that fits the memory budget is used (B = bmax ~ n^(1/(L+1)),
 // 2 L B + 2 bmax + 3 native vectors, L + 1 replays of the run).  The adjoint vectors and every
 // dot product are FP64 (10 FP64 work vectors).
+//
+// A reverse step does not synchronise with the host: its dot products and bbar stay in device
+// memory and feed the step kernels directly, and for systems with the Gram path (ordr <= 2)
+// the adjoint's Gram matrices are summed on the device over all steps, the gradient being
+// assembled once at the end (it is linear in them).  Cubic and quartic systems contract
+// d<wbar|H|v_i>/dtheta per step on the host side of nvb_hv_adjoint_coeffs.
 #include <cuda_runtime.h>
 
 #include <algorithm>
