@@ -377,6 +377,17 @@ def large_cubic(dev: int, iters: int = 4, warm: int = 2, grad_iters: int = 60, b
     return out
 
 
+def workload_name(cfgn: int, basis=None) -> str:
+    """The benchmark system's description as both arms' JSON lines name it."""
+    import math
+    from nadvibs_b200 import synth
+    cfg = synth.config(cfgn)
+    basis = list(basis) if basis else list(cfg.basis)
+    n = math.prod(basis) * cfg.nstates
+    return (f"config{cfgn}: {cfg.nstates} states, {cfg.nmodes} modes, basis [{','.join(str(b) for b in basis)}], "
+            f"{n:,} functions, ordr {cfg.ordr}, plain Lanczos (reorthog=0)")
+
+
 def hv_flops(cfg) -> float:
     """Reference-equivalent arithmetic of one H.v, from the term table (the reference's pass
     structure, Source/top.f90:717-806): 2 flops per row for every nonzero (monomial, nonzero
@@ -436,8 +447,8 @@ def main():
         line = {"metric": METRIC, "value": cb["value"], "unit": "iter/s", "impl": "reference", "n_gpus": args.gpus,
                 "steps": iters, "warmup": 0, "ms_per_step": 1e3 / cb["value"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "config2: 3 states, basis [20,16,12,10,8,8,6,6], 265,420,800 functions, "
-                                       "ordr 2, plain Lanczos", "precision": "fp64", "cache": "inputs larger than L2"},
+                "config": {"workload": workload_name(args.config), "precision": "fp64",
+                           "cache": "inputs larger than L2" if args.config in (2, 3, 5) else "inputs in L2"},
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "iter/s", "h2d_bytes_per_step": 0,
                                             "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -459,9 +470,8 @@ def main():
         "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if main_prec == "fp64" else "f32+f64",
-        "data": "synthetic (seeded basis.in/nadvibs.in, numpy default_rng(1002))",
-        "config": {"workload": "config2: 3 states, 8 modes, basis [20,16,12,10,8,8,6,6], 265,420,800 functions, "
-                               "ordr 2, plain Lanczos (reorthog=0)", "precision": main_prec,
+        "data": f"synthetic (seeded basis.in/nadvibs.in, numpy default_rng({cfg.seed}))",
+        "config": {"workload": workload_name(args.config, cfg.basis), "precision": main_prec,
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "cache": "inputs larger than L2 (2.1 GB FP64 vectors), no flush"},
         "roofline": {"bound": "hbm", "achieved": hv_gbs, "peak": peak, "unit": "GB/s", "frac": hv_gbs / peak,
