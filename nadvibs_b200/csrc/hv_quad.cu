@@ -15,8 +15,8 @@
 //   slow pairs:   y_a += Q^a_kl e x_a(p+-e_k+-e_l);
 // with e the tile's slow element factor.  Finally y_a += X_l Z_l: by register shifts for
 // l = m, and for each other fast mode through one shared-memory buffer (one mode at a time,
-// so that the buffer costs one ring slot, not NF - 1).  Out-of-basis neighbours have element factor 0
-// (the item is skipped by producer and consumers alike) and zero-filled halos.
+// so that the buffer costs one ring slot, not NF - 1).  Out-of-basis neighbours have element
+// factor 0 (the item is skipped by producer and consumers alike) and zero-filled halos.
 // Every wait is bounded: a wait that runs out raises a CTA abort flag, after which no thread
 // waits again and the kernel reports the failure through its error word.
 #include <cuda_runtime.h>
