@@ -302,8 +302,9 @@ int nvb_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, i
  * library (4097 doubles, ~32 KiB per GPU that loads it, kept until exit), so n <= 2^32
  * (larger n fails with NVB_ERR_ARG).  All calls share that array and each overwrites the
  * partials it reads; calls that overlap on the GPU race, so order them (one stream or
- * events).  The first call on each device looks up the array's address
- * (cudaGetSymbolAddress, once per device) and should come before any stream capture. */
+ * events).  The grid is sized from n (up to eight blocks per multiprocessor).  The first call
+ * on each device looks up the array's address (cudaGetSymbolAddress, once per device and
+ * again after a reset of the device's context) and should come before any stream capture. */
 int nvb_dot_noalloc(const void *a, double sa, const void *b, double sb, int64_t n, int64_t dtype, double *result_dev,
                     void *stream);
 

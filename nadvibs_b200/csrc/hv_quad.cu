@@ -234,6 +234,12 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                 const long long tb = (long long)tile * TF;
                 for (int i = 0; i < cnt && !stop; ++i) {
                     const QuadItem qi = s_it[pl[1 + i]];
+                    // after an abort no new copy is issued: a consumer that gave up does not
+                    // release its slot, but a slot released earlier may still look free
+                    if (*abort_flag) {
+                        stop = 1;
+                        break;
+                    }
                     if (mbar_wait(&empty[slot], ph ^ 1u, abort_flag, A.wait_limit)) {
                         mbar_expect_tx(&full[slot], bytes);
                         bulk_g2s(s_ring + slot * sst + pad, x + qi.b * N + tb + (long long)qi.tshift * TF, bytes,
@@ -295,11 +301,14 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
         ok = mbar_try(&full[slot], ph) || mbar_wait(&full[slot], ph, abort_flag, A.wait_limit);
         return s_ring + slot * sst + pad + tid;
     };
-    // hand the slot back to the producer (one arrival per warp) and step to the next one
+    // hand the slot back to the producer (one arrival per warp, by lane 0) and step to the
+    // next one.  Only a lane 0 that saw the slot's copy land releases it: a slot whose wait
+    // gave up may still be the target of a copy in flight, so it is never handed back (the
+    // producer then stops on the abort flag and drains its copies before the CTA exits).
     auto release = [&]() {
         __syncwarp();
-        if constexpr (kNoBranch) mbar_arrive_if(&empty[slot], lane == 0);
-        else if (lane == 0) mbar_arrive(&empty[slot]);
+        if constexpr (kNoBranch) mbar_arrive_if(&empty[slot], lane == 0 && ok);
+        else if (lane == 0 && ok) mbar_arrive(&empty[slot]);
         if (++slot == NS) {
             slot = 0;
             ph ^= 1u;
@@ -568,8 +577,8 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                         for (int r = 0; r < R; ++r) acc[r] = fma(c1, v1[r], fma(c0, v0[r], acc[r]));
                     }
                     __syncwarp();
-                    if constexpr (kNoBranch) mbar_arrive_if(&empty[s0], lane == 0);
-                    else if (lane == 0) mbar_arrive(&empty[s0]);
+                    if constexpr (kNoBranch) mbar_arrive_if(&empty[s0], lane == 0 && ok0);
+                    else if (lane == 0 && ok0) mbar_arrive(&empty[s0]);
                     release();
                 }
                 if (j < nsp) {

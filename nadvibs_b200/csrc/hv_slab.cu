@@ -271,7 +271,10 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
     bool failed = false;
     while (g >= 0) {
         do_direct(quota);
-        if (!mbar_wait(&bar[bi], (phase_bits >> bi) & 1u)) {
+        // the decision to give up is block-wide: every thread leaves the loop together (its
+        // barriers stay uniform), and the copies still in flight are drained below
+        const bool landed = mbar_wait(&bar[bi], (phase_bits >> bi) & 1u);
+        if (__syncthreads_or(!landed)) {
             failed = true;
             break;
         }
@@ -408,7 +411,14 @@ __global__ void __launch_bounds__(SlabMaxThreads<T>::value) k_hv_slab(SlabArgs<T
         bi ^= 1;
     }
     if (failed) {
-        if (tid == 0) atomicExch(A.err, 1);
+        if (tid == 0) {
+            // buffer bi holds the copy that was awaited, buffer bi^1 the next group's copy
+            // (issued when there is one): wait for both (bounded) before the CTA leaves, so
+            // that no bulk copy completes into the shared memory of an exited CTA
+            mbar_wait(&bar[bi], (phase_bits >> bi) & 1u);
+            if (nxt >= 0) mbar_wait(&bar[bi ^ 1], (phase_bits >> (bi ^ 1)) & 1u);
+            atomicExch(A.err, 1);
+        }
         return;
     }
     do_direct(A.ngroups);

@@ -12,8 +12,9 @@
  *
  * Deviations from the reference's arithmetic, all at the rounding level:
  *  - the reference forms the harmonic energy (dkin) and the matrix-element product d1
- *    incrementally along its row sweep (Source/top.f90:721-730, 794-796); here both
- *    are formed directly per row;
+ *    incrementally along its row sweep (Source/top.f90:721-730, 794-796); here dkin is
+ *    formed directly per row, and d1 is recomputed from scratch whenever the row walk
+ *    changes one of the term's digits (the walk itself is incremental, as the reference's);
  *  - GA_DDOT's reduction order is rank dependent; here dots are summed in row order
  *    (single thread) or per-thread blocks combined in thread order (OpenMP).
  * The per-element accumulation order of H.v follows the reference: diagonal part first,
@@ -122,8 +123,13 @@ static int is_diag_term(const orc_system *S, int64_t t)
     return 1;
 }
 
-/* y = H x, layout x[s*dimen + r] (column-major q(dimen,nstates)).  Source/top.f90:672-818. */
-int orc_hv(const orc_system *S, const double *x, double *y, int nthreads)
+/* y = H x, layout x[s*dimen + r] (column-major q(dimen,nstates)).  Source/top.f90:672-818.
+ * walk = 1: each (term, shift) pass walks its rows with an incremental mixed-radix counter of
+ * the digits (Source/top.f90:781-803: a per-row increment of the fastest digit with carries;
+ * the element product of the term is recomputed only when one of the term's digits changed);
+ * walk = 0: the digits of every row are decoded by division in every pass.  Both give the same
+ * bits (same products in the same order per element); walk = 1 is the timed CPU baseline. */
+static int orc_hv_impl(const orc_system *S, const double *x, double *y, int nthreads, int walk)
 {
     const int64_t N = orc_dimen(S), NS = S->nstates, M = S->nmodes;
     int64_t shft[ORC_MAXM];
@@ -204,6 +210,46 @@ int orc_hv(const orc_system *S, const double *x, double *y, int nthreads)
             const double *pc = S->tcoef + t * S->maxpairs;
             int64_t sd[8];
             for (int64_t q = 0; q < d; ++q) sd[q] = sdir[q];
+            if (walk) {
+                int64_t mdmax = 0;
+                for (int64_t q = 0; q < d; ++q) mdmax = md[q] > mdmax ? md[q] : mdmax;
+#pragma omp parallel
+                {
+                    int nth = 1, tid = 0;
+#ifdef _OPENMP
+                    nth = omp_get_num_threads();
+                    tid = omp_get_thread_num();
+#endif
+                    const int64_t r0 = N * tid / nth, r1 = N * (tid + 1) / nth;
+                    int64_t n[ORC_MAXM];
+                    int64_t rem = r0;
+                    for (int64_t k = 0; k < M; ++k) { n[k] = rem / shft[k]; rem -= n[k] * shft[k]; }
+                    int dirty = 1, ok = 0;
+                    double d1 = 1.0;
+                    for (int64_t r = r0; r < r1; ++r) {
+                        if (dirty) {
+                            d1 = 1.0;
+                            ok = 1;
+                            for (int64_t q = 0; q < d; ++q) {
+                                int64_t nc = n[md[q]] + sd[q];
+                                if (nc < 0 || nc >= S->nfunc[md[q]]) { ok = 0; break; }
+                                d1 = d1 * elem(S, pw[q], n[md[q]], sd[q]);
+                            }
+                            dirty = 0;
+                        }
+                        if (ok) {
+                            int64_t c = r + stride;
+                            for (int64_t q = 0; q < np; ++q)
+                                y[(pa[q] - 1) * N + r] = y[(pa[q] - 1) * N + r] + x[(pb[q] - 1) * N + c] * pc[q] * d1;
+                        }
+                        /* next row: increment the fastest digit, carrying into slower ones */
+                        int64_t k = M - 1;
+                        while (k >= 0 && ++n[k] == S->nfunc[k]) { n[k] = 0; --k; }
+                        if (k <= mdmax) dirty = 1;
+                    }
+                }
+                continue;
+            }
 #pragma omp parallel for schedule(static)
             for (int64_t r = 0; r < N; ++r) {
                 double d1 = 1.0;
@@ -222,6 +268,17 @@ int orc_hv(const orc_system *S, const double *x, double *y, int nthreads)
         }
     }
     return 0;
+}
+
+int orc_hv(const orc_system *S, const double *x, double *y, int nthreads)
+{
+    return orc_hv_impl(S, x, y, nthreads, 1);
+}
+
+/* the same product with the digits of every row decoded by division in every pass */
+int orc_hv_rowdiv(const orc_system *S, const double *x, double *y, int nthreads)
+{
+    return orc_hv_impl(S, x, y, nthreads, 0);
 }
 
 /* y at selected rows only (all states), same terms as orc_hv, for full-size spot checks:

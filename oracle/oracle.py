@@ -100,11 +100,14 @@ class OracleSystem:
     def ntotal(self) -> int:
         return self.dimen * self.nstates
 
-    def hv(self, x: np.ndarray, nthreads: int = 1) -> np.ndarray:
+    def hv(self, x: np.ndarray, nthreads: int = 1, rowdiv: bool = False) -> np.ndarray:
+        """y = H x.  rowdiv=True decodes every row's digits by division in every pass instead
+        of walking them with the incremental counter (same result, bit for bit)."""
         x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
         assert x.size == self.ntotal
         y = np.empty_like(x)
-        rc = lib().orc_hv(C.byref(self.s), _p(x), _p(y), C.c_int(nthreads))
+        fn = lib().orc_hv_rowdiv if rowdiv else lib().orc_hv
+        rc = fn(C.byref(self.s), _p(x), _p(y), C.c_int(nthreads))
         if rc:
             raise RuntimeError(f"orc_hv failed {rc}")
         return y

@@ -6,13 +6,15 @@ spectra ``output`` / ``output.adia`` produced from them by ``convolve/main.f90``
 grid -0.1..0.4 eV with 2002 points, shift 2.7807 eV).  This script copies those numbers
 into JSON so the tests can run without the reference checkout.
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py <path of the reference checkout>
 """
 import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py <path of the reference checkout>")
+ref = sys.argv[1]
 here = os.path.dirname(os.path.abspath(__file__))
 
 

@@ -144,29 +144,36 @@ def test_hv_benchmark_systems_full(n):
 
 
 @pytest.mark.parametrize("n", [2])
-def test_hv_drop_in_size_rows_and_symmetry(n):
-    """Full-size systems: oracle rows at 2000 random positions (plus the first/last rows and
-    the truncation corners), and <u,Hv> = <Hu,v> over the whole vector."""
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_hv_drop_in_size_rows_and_symmetry(n, dt):
+    """Full-size systems through the benchmark's kernel in both precisions: oracle rows at 2000
+    random positions (plus the first/last rows and the truncation corners) of H x for the
+    same (FP32-rounded, for FP32) x, and <u,Hv> = <Hu,v> over the whole vector."""
     cfg = synth.config(n)
     om, cc, pot = synth.draw(cfg)
     S = O.system_from_arrays(cfg.basis, cfg.nstates, cfg.ordr, om, cc, pot)
     N = S.dimen
+    code = L.DTYPE_F64 if dt == torch.float64 else L.DTYPE_F32
+    tol = TOL64 if dt == torch.float64 else TOL32
     g = torch.Generator(device="cuda").manual_seed(n)
-    x = torch.randn(S.ntotal, generator=g, device="cuda", dtype=torch.float64)
-    u = torch.randn(S.ntotal, generator=g, device="cuda", dtype=torch.float64)
+    x = torch.randn(S.ntotal, generator=g, device="cuda", dtype=dt)
+    u = torch.randn(S.ntotal, generator=g, device="cuda", dtype=dt)
     with _handle(_params(cfg), om, cc, pot) as h:
+        assert h.hv_kernel(code) == "quad"
         h.set_stream(torch.cuda.current_stream().cuda_stream)
         y = torch.empty_like(x)
-        h.hv_ptr(x.data_ptr(), y.data_ptr(), L.DTYPE_F64)
+        h.hv_ptr(x.data_ptr(), y.data_ptr(), code)
         hu = torch.empty_like(u)
-        h.hv_ptr(u.data_ptr(), hu.data_ptr(), L.DTYPE_F64)
+        h.hv_ptr(u.data_ptr(), hu.data_ptr(), code)
         torch.cuda.synchronize()
-        lhs = torch.dot(u, y).item()
-        rhs = torch.dot(hu, x).item()
-        assert abs(lhs - rhs) <= 1e-10 * torch.linalg.vector_norm(y).item() * torch.linalg.vector_norm(u).item()
+        lhs = torch.dot(u.double(), y.double()).item()
+        rhs = torch.dot(hu.double(), x.double()).item()
+        sym_tol = 1e-10 if dt == torch.float64 else 1e-5
+        assert abs(lhs - rhs) <= sym_tol * torch.linalg.vector_norm(y.double()).item() * \
+            torch.linalg.vector_norm(u.double()).item()
         rng = np.random.default_rng(n)
         rows = np.concatenate([[0, 1, N - 2, N - 1], rng.integers(0, N, size=2000)])
-        xh = x.cpu().numpy()
+        xh = x.double().cpu().numpy()
         yr = S.hv_rows(xh, rows)
-        yg = y.view(cfg.nstates, N).cpu().numpy()[:, rows].T
-        assert np.abs(yg - yr).max() <= TOL64 * np.abs(yr).max()
+        yg = y.view(cfg.nstates, N).double().cpu().numpy()[:, rows].T
+        assert np.abs(yg - yr).max() <= tol * np.abs(yr).max()

@@ -212,3 +212,25 @@ def test_convolution_reproduces_reference_fixture(oracle_lib, name):
     assert len(xo) == len(spec)
     assert np.abs(xo - spec[:, 0]).max() <= 5.01e-9   # printed with 8 decimals (f15.8)
     assert np.abs(yo - spec[:, 1]).max() <= 5.01e-9
+
+
+@pytest.mark.parametrize("case", [("cfg", 1), ("small", (8, 3, [2, 3, 2], 3)), ("small", (16, 5, [2, 2, 2, 2, 2, 2], 3)),
+                                  ("small", (15, 3, [6, 5, 4], 4))])
+@pytest.mark.parametrize("nthreads", [1, 3])
+def test_oracle_counter_walk_equals_per_row_division(case, nthreads):
+    """The timed H.v pass walks rows with an incremental mixed-radix counter (as
+    Source/top.f90:781-803 does); it gives the same bits as decoding every row by division."""
+    kind, arg = case
+    if kind == "cfg":
+        cfg = synth.config(arg)
+        om, cc, pot = synth.draw(cfg)
+        S = O.system_from_arrays(cfg.basis, cfg.nstates, cfg.ordr, om, cc, pot)
+    else:
+        seed, ns, basis, ordr = arg
+        cfg = synth.random_small(seed, ns, basis, ordr)
+        om, cc, pot = synth.draw_small(cfg)
+        S = O.system_from_arrays(basis, ns, ordr, om, cc, pot)
+    x = np.random.default_rng(7).normal(size=S.ntotal)
+    a = S.hv(x, nthreads=nthreads)
+    b = S.hv(x, nthreads=nthreads, rowdiv=True)
+    assert np.array_equal(a, b)
