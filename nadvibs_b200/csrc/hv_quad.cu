@@ -234,12 +234,11 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                 const long long tb = (long long)tile * TF;
                 for (int i = 0; i < cnt && !stop; ++i) {
                     const QuadItem qi = s_it[pl[1 + i]];
-                    // after an abort no new copy is issued: a consumer that gave up does not
-                    // release its slot, but a slot released earlier may still look free
-                    if (*abort_flag) {
-                        stop = 1;
-                        break;
-                    }
+                    // No slot whose copy may still be in flight is ever free here: a consumer
+                    // whose wait gave up does not release its slot, so the producer's wait for
+                    // that slot runs out (or sees the abort flag) and it stops.  (Reading the
+                    // abort flag before every copy as well costs ~20 % of the kernel time: the
+                    // producer lane is on the critical path.)
                     if (mbar_wait(&empty[slot], ph ^ 1u, abort_flag, A.wait_limit)) {
                         mbar_expect_tx(&full[slot], bytes);
                         bulk_g2s(s_ring + slot * sst + pad, x + qi.b * N + tb + (long long)qi.tshift * TF, bytes,
@@ -272,18 +271,30 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
     }
 
     // ---------------- consumers ----------------
+    // the thread's digits and ladder factors along the fast modes j >= 1; FP64 reads the factors
+    // from the element table when used (registers are its limit: 168 per thread at 10 warps)
     int dj[NF];
-    T e1p[NF], e1m[NF];
+    T e1pa[NF], e1ma[NF];
 #pragma unroll
     for (int j = 0; j < NF; ++j) {
         dj[j] = 0;
-        e1p[j] = e1m[j] = (T)0;
+        e1pa[j] = e1ma[j] = (T)0;
         if (j >= 1) {
             dj[j] = (tid / F.sh[j]) % F.nf[j];
-            e1p[j] = s_tab[((m + j) * 5 + 0) * nmax + dj[j]];
-            e1m[j] = s_tab[((m + j) * 5 + 1) * nmax + dj[j]];
+            if constexpr (sizeof(T) == 4) {
+                e1pa[j] = s_tab[((m + j) * 5 + 0) * nmax + dj[j]];
+                e1ma[j] = s_tab[((m + j) * 5 + 1) * nmax + dj[j]];
+            }
         }
     }
+    auto e1p = [&](int j) -> T {
+        if constexpr (sizeof(T) == 8) return s_tab[((m + j) * 5 + 0) * nmax + dj[j]];
+        else return e1pa[j];
+    };
+    auto e1m = [&](int j) -> T {
+        if constexpr (sizeof(T) == 8) return s_tab[((m + j) * 5 + 1) * nmax + dj[j]];
+        else return e1ma[j];
+    };
     const T sc = scale_dev ? (T)(*scale_dev) : (T)1;
     const int nv = A.nv;
     const int lane = tid & 31, wid = tid >> 5;
@@ -400,9 +411,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
 #pragma unroll
                 for (int j = 0; j < NF; ++j) Z[j][r] = (T)0;
             }
-            T hj[NF];  // <n|x^2|n> of the thread's fast digits (j >= 1)
-#pragma unroll
-            for (int j = 0; j < NF; ++j) hj[j] = (T)dj[j] + (T)0.5;
+            auto hj = [&](int j) -> T { return (T)dj[j] + (T)0.5; };  // <n|x^2|n> of the fast digit j >= 1
             // own tile x_a: diagonal section, fast linear and bilinear into Z, fast squares
             {
                 const T *buf = take();
@@ -412,8 +421,8 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                     T ek = dt[SS], daa = dt[a * S + a];
 #pragma unroll
                     for (int j = 1; j < NF; ++j) {
-                        ek += F.om[j] * hj[j];
-                        daa += F.R[j][a][a] * hj[j];
+                        ek += F.om[j] * hj(j);
+                        daa += F.R[j][a][a] * hj(j);
                     }
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
@@ -445,7 +454,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                                 V[r] = v;
                             } else {
                                 const T *p = buf + r * nc;
-                                V[r] = e1p[i] * p[F.sh[i]] + e1m[i] * p[-F.sh[i]];
+                                V[r] = e1p(i) * p[F.sh[i]] + e1m(i) * p[-F.sh[i]];
                             }
                         }
 #pragma unroll
@@ -494,7 +503,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                     if ((A.dpm >> (a * S + b)) & 1u) {
                         T dab = dt[a * S + b];
 #pragma unroll
-                        for (int j = 1; j < NF; ++j) dab += F.R[j][a][b] * hj[j];
+                        for (int j = 1; j < NF; ++j) dab += F.R[j][a][b] * hj(j);
                         const T r0 = F.R[0][a][b];
 #pragma unroll
                         for (int r = 0; r < R; ++r) acc[r] += (dab + r0 * ((T)r + (T)0.5)) * xb[r];
@@ -608,7 +617,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const T *p = s_z + pad + r * nc + tid;
-                    acc[r] += e1p[j] * p[F.sh[j]] + e1m[j] * p[-F.sh[j]];
+                    acc[r] += e1p(j) * p[F.sh[j]] + e1m(j) * p[-F.sh[j]];
                 }
                 consumer_sync(nc);  // s_z is rewritten next
             }
