@@ -251,8 +251,11 @@ int nvb_seed_overlap(nvb_handle *h, double *overlap);
 
 /* Record checkpoints of the forward for nvb_lanczos_backward: from the next nvb_seed on,
  * nvb_lanczos saves (v_{c-1}, v_c) at iterations c = 1, 1+k, 1+2k, ... in device memory
- * (2 ceil(niter/k) vectors of the handle's precision).  k = 0 stops recording and frees them.
- * No reference counterpart. */
+ * (2 ceil(niter/k) vectors of the handle's precision).  k = -1 records the whole forward
+ * (every v_j and w_j = H v_j, 2 niter + 2 vectors) when that and the sweep's work vectors fit
+ * the budget of nvb_set_backward_memory, and nothing otherwise; a sweep with k = -1 then
+ * replays nothing (or, without the record, takes the automatic plan of k = 0).  k = 0 stops
+ * recording and frees them.  No reference counterpart. */
 int nvb_set_checkpoints(nvb_handle *h, int64_t k);
 
 /* Reverse sweep through the first n Lanczos iterations (plain Lanczos, reorthog = 0): given
@@ -263,6 +266,8 @@ int nvb_set_checkpoints(nvb_handle *h, int64_t k);
  *   k > 0: one level, pairs every k iterations (the forward's, when nvb_set_checkpoints(h, k)
  *          preceded nvb_seed; else one replay from the seed records them), each range of k
  *          iterations replayed into storage (2k + 3 vectors of the handle's precision);
+ *   k = -1: the forward's full record (nvb_set_checkpoints(h, -1)), nothing replayed; the
+ *          automatic plan when the record was not kept;
  *   k = 0: automatic.  The shallowest recursion that fits the budget of
  *          nvb_set_backward_memory (default 85% of free device memory): with depth L, each
  *          level splits its range into B ~ n^(1/(L+1)) sub-ranges whose starting pairs one

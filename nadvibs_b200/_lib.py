@@ -346,7 +346,8 @@ class Handle:
         check(lib().nvb_set_fault_test(self.ptr, mode))
 
     def set_checkpoints(self, k: int):
-        """Record (v_{c-1}, v_c) every k iterations from the next seed (nvb_set_checkpoints)."""
+        """Record (v_{c-1}, v_c) every k iterations from the next seed (nvb_set_checkpoints);
+        k = -1 records the whole forward when it fits the backward budget."""
         check(lib().nvb_set_checkpoints(self.ptr, k))
 
     def set_backward_memory(self, nbytes: int):

@@ -19,9 +19,18 @@ dL/dbeta_i,
 with Sbar = e_1 (2 s_1 Ibar)^T; pairs of nearly equal Ritz values (ghost copies of a
 converged root) are damped, F_ij = d/(d^2 + eps^2).  Then ``nvb_lanczos_backward`` runs the
 reverse sweep through the recurrence on the GPU and contracts the adjoint vectors with
-dH/dtheta.  The primal vectors are recomputed from checkpoint pairs: with k > 0 one level every
-k iterations; with k = 0 (the default) the shallowest recursive checkpointing that fits the
-device-memory budget (``Handle.set_backward_memory``; everything stored when it fits).
+dH/dtheta.  The primal vectors come from the forward: with k = -1 (the default) the forward
+records every v_j and H v_j when they fit the device-memory budget
+(``Handle.set_backward_memory``) and the sweep replays nothing; otherwise they are recomputed
+from checkpoint pairs: with k > 0 one level every k iterations; with k = 0 (or -1 without the
+record) the shallowest recursive checkpointing that fits the budget.
+
+Losses: after a long plain-Lanczos run the unconverged Ritz values are chaotic functions of
+theta at the scale of rounding (ghost copies form as roots converge), so a loss over all Ritz
+values has no finite-difference limit.  ``ritz(..., residuals=True)`` also returns the
+residual estimates bji; ``converged_mask`` / ``converged_spectrum`` restrict a loss to the
+converged roots (ghost copies included), a smooth function of theta whose reverse-sweep
+gradient agrees with central differences.
 """
 from __future__ import annotations
 
@@ -83,7 +92,8 @@ def tridiag_eig_backward(E: np.ndarray, S: np.ndarray, gE: np.ndarray | None, gI
 
 
 class LanczosRitz(torch.autograd.Function):
-    """(E, I) = Ritz energies and intensities of niter Lanczos steps on H(theta)."""
+    """(E, I, bji) = Ritz energies, intensities and residual estimates |beta_n s_{n,i}| of niter
+    Lanczos steps on H(theta); bji is not differentiable (it selects converged roots)."""
 
     @staticmethod
     def forward(ctx, theta: torch.Tensor, params, niter: int, k: int, opts: dict):
@@ -103,10 +113,12 @@ class LanczosRitz(torch.autograd.Function):
         ctx.dev = theta.device
         out_E = torch.from_numpy(E.copy()).to(theta.device)
         out_I = torch.from_numpy((S[0, :] ** 2).copy()).to(theta.device)
-        return out_E, out_I
+        out_r = torch.from_numpy(np.abs(b[niter] * S[-1, :])).to(theta.device)
+        ctx.mark_non_differentiable(out_r)
+        return out_E, out_I, out_r
 
     @staticmethod
-    def backward(ctx, gE, gI):
+    def backward(ctx, gE, gI, gR=None):
         gEn = None if gE is None else gE.detach().to("cpu", torch.float64).numpy()
         gIn = None if gI is None else gI.detach().to("cpu", torch.float64).numpy()
         dev = ctx.dev if torch.device(ctx.dev).type == "cuda" else None
@@ -122,9 +134,33 @@ class LanczosRitz(torch.autograd.Function):
         return torch.from_numpy(g).to(ctx.dev), None, None, None, None
 
 
-def ritz(theta: torch.Tensor, params, niter: int, k: int = 0, **opts):
-    """Differentiable Ritz energies (hartree) and intensities of niter Lanczos steps."""
-    return LanczosRitz.apply(theta, params, niter, k, opts)
+def ritz(theta: torch.Tensor, params, niter: int, k: int = -1, residuals: bool = False, **opts):
+    """Differentiable Ritz energies (hartree) and intensities of niter Lanczos steps (k: the
+    checkpoint interval of nvb_set_checkpoints; the default -1 records the whole forward when
+    it fits the backward budget, so the reverse sweep replays nothing, and otherwise takes the
+    automatic recursive plan); with
+    residuals=True also the residual estimates bji = |beta_n s_{n,i}| (hartree, constant
+    w.r.t. theta), the convergence test of the reference's eigenvalue table
+    (Source/top.f90:1074)."""
+    E, I, r = LanczosRitz.apply(theta, params, niter, k, opts)
+    return (E, I, r) if residuals else (E, I)
+
+
+def converged_mask(bji: torch.Tensor, tol: float = 1e-9) -> torch.Tensor:
+    """Ritz values converged to tol (bji < tol, hartree), ghost copies of converged roots
+    included.  A spectrum or loss restricted to them is a smooth function of theta: after a
+    long plain-Lanczos run the unconverged Ritz values are chaotic at the scale of rounding
+    (finite differences of them do not converge as the step shrinks), while a converged root,
+    summed over its ghost copies, has a well-defined energy and Franck-Condon weight.  Use the
+    mask of the unperturbed run as a constant when comparing with finite differences."""
+    return bji < tol
+
+
+def converged_spectrum(E: torch.Tensor, I: torch.Tensor, mask: torch.Tensor, grid_cm: torch.Tensor,
+                       sigma_cm: float = 20.0) -> torch.Tensor:
+    """Gaussian-broadened spectrum of the converged Ritz values (mask from converged_mask),
+    energies relative to the lowest of them (cm^-1)."""
+    return convolved_spectrum(E[mask], I[mask], grid_cm, sigma_cm)
 
 
 def convolved_spectrum(E: torch.Tensor, I: torch.Tensor, grid_cm: torch.Tensor, sigma_cm: float = 20.0,

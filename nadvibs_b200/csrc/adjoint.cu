@@ -177,16 +177,17 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_diag(const long long *__res
 
 constexpr int GRAM_TR = 64;      // rows per shared-memory tile (a multiple of 4)
 static_assert(GRAM_TR % 4 == 0, "the Gram sums are unrolled by 4 rows");
-constexpr int GRAM_MAXPER = 8;   // Gram outputs per thread: S*(3M+1)*S + (MS)^2 <= 8*256
+constexpr int GRAM_MAXPER = 8;   // Gram outputs: S*(3M+1)*S + (MS)^2 <= 8*256 (4-output tasks <= 256 threads)
 
 // Per block: for each tile of GRAM_TR rows, the expanded columns of those rows go to shared
 // memory (one thread per (row, state)), then every thread accumulates its Gram outputs over
 // the tile.  Outputs o < n1: G1[a][j] = <u_a, B_j>; o >= n1: G2[(k,a)][(l,b)] = <X_k u_a, X_l v_b>.
 template <typename T>
-__global__ void __launch_bounds__(256) k_adj_gram(const T *__restrict__ u, const T *__restrict__ v,
+__global__ void __launch_bounds__(256, 4) k_adj_gram(const T *__restrict__ u, const T *__restrict__ v,
                                                  const double *__restrict__ etab, int nmax,
                                                  const int *__restrict__ nfunc, const long long *__restrict__ shft,
-                                                 int M, int S, long long dimen, double *__restrict__ part) {
+                                                 int M, int S, long long dimen, int accumulate,
+                                                 double *__restrict__ part) {
     extern __shared__ double sm[];
     const int MS = M * S, nA = S + MS, nB = S + 3 * MS;
     const int n1 = S * nB, n2 = MS * MS, nout = n1 + n2;
@@ -196,9 +197,30 @@ __global__ void __launch_bounds__(256) k_adj_gram(const T *__restrict__ u, const
     const double *D2 = etab + (1 * ETAB_J + 0) * nmax;  // <m|x^2|m>
     const int tid = threadIdx.x, nth = blockDim.x;
     const bool small = dimen <= 0xFFFFFFFFll;
-    double acc[GRAM_MAXPER];
-#pragma unroll
-    for (int q = 0; q < GRAM_MAXPER; ++q) acc[q] = 0.0;
+    // this thread's task: 4 outputs of one row ia of G1 or G2, and its row group
+    const int K1 = (nB + 3) / 4, K2 = (MS + 3) / 4;
+    const int ntask = S * K1 + MS * K2;
+    const int ngrp = nth / ntask > 0 ? nth / ntask : 1;  // row groups splitting the tile
+    const int task = tid % ntask, rg = tid / ntask;
+    int ia, jb0, kst, nq, obase;
+    if (task < S * K1) {
+        ia = task / K1;
+        const int k = task - ia * K1;
+        jb0 = k;
+        kst = K1;
+        nq = k + 3 * K1 < nB ? 4 : (nB - k + K1 - 1) / K1;
+        obase = ia * nB + k;
+    } else {
+        const int t2 = task - S * K1;
+        const int i2 = t2 / K2, k = t2 - i2 * K2;
+        ia = S + i2;
+        jb0 = S + k;
+        kst = K2;
+        nq = k + 3 * K2 < MS ? 4 : (MS - k + K2 - 1) / K2;
+        obase = n1 + i2 * MS + k;
+    }
+    const int active_rg = rg < ngrp;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (long long t0 = (long long)blockIdx.x * GRAM_TR; t0 < dimen; t0 += (long long)gridDim.x * GRAM_TR) {
         for (int e = tid; e < GRAM_TR * S; e += nth) {
             const int rl = e % GRAM_TR, s = e / GRAM_TR;
@@ -244,53 +266,65 @@ __global__ void __launch_bounds__(256) k_adj_gram(const T *__restrict__ u, const
             }
         }
         __syncthreads();
+        // G1 row ia < S: tasks k < K1, outputs jb = k + q K1 (q < 4) of the nB columns of B;
+        // G2 row ia >= S: tasks k < K2, outputs jb = S + k + q K2 of the MS columns X v.  Lanes
+        // of a task row read consecutive words of sB; the row groups split the tile's rows.
+        if (task < ntask && active_rg) {
+            const double *pa = sA + ia;
+            const double *pb = sB + jb0;
+            for (int r = rg; r < GRAM_TR; r += ngrp) {
+                const double a = pa[r * nA];
+                const double *b = pb + r * nB;
 #pragma unroll
-        for (int q = 0; q < GRAM_MAXPER; ++q) {
-            const int o = tid + q * nth;
-            if (o < nout) {
-                int ia, jb;
-                if (o < n1) {
-                    ia = o / nB;
-                    jb = o - ia * nB;
-                } else {
-                    const int o2 = o - n1;
-                    ia = S + o2 / MS;
-                    jb = S + (o2 - (o2 / MS) * MS);
-                }
-                // four independent partial sums: the FMA chain of one output is the latency
-                double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
-#pragma unroll 4
-                for (int r = 0; r < GRAM_TR; r += 4) {
-                    x0 += sA[r * nA + ia] * sB[r * nB + jb];
-                    x1 += sA[(r + 1) * nA + ia] * sB[(r + 1) * nB + jb];
-                    x2 += sA[(r + 2) * nA + ia] * sB[(r + 2) * nB + jb];
-                    x3 += sA[(r + 3) * nA + ia] * sB[(r + 3) * nB + jb];
-                }
-                acc[q] += (x0 + x1) + (x2 + x3);
+                for (int q = 0; q < 4; ++q)
+                    if (q < nq) acc[q] += a * b[q * kst];
             }
         }
         __syncthreads();
     }
+    // sum the row groups' partials (in group order) and update the block's partials:
+    // overwritten, or (accumulate) summed over the calls of a reverse sweep by the block that
+    // owns them, so one reduction over blocks serves all its steps
+    double *red = sm;  // reuses the tile: [ngrp][ntask][4]
+    if (task < ntask && active_rg)
 #pragma unroll
-    for (int q = 0; q < GRAM_MAXPER; ++q) {
-        const int o = tid + q * nth;
-        if (o < nout) part[(long long)blockIdx.x * nout + o] = acc[q];
+        for (int q = 0; q < 4; ++q) red[(rg * ntask + task) * 4 + q] = acc[q];
+    __syncthreads();
+    if (task < ntask && rg == 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (q >= nq) break;
+            double v = 0.0;
+            for (int g2 = 0; g2 < ngrp; ++g2) v += red[(g2 * ntask + task) * 4 + q];
+            double *pp = part + (long long)blockIdx.x * nout + obase + q * kst;
+            *pp = accumulate ? *pp + v : v;
+        }
     }
 }
 
-static bool gram_fits(int S, int M) {
+// shared memory of one Gram block: the expanded tile, or the row groups' partials at the end
+static size_t gram_smem(int S, int M) {
     const int MS = M * S, nA = S + MS, nB = S + 3 * MS;
-    return S * nB + MS * MS <= GRAM_MAXPER * 256 && (size_t)GRAM_TR * (nA + nB) * sizeof(double) <= 200 * 1024;
+    return std::max<size_t>((size_t)GRAM_TR * (nA + nB), 4 * 256) * sizeof(double);
 }
 
-// out[o] (+)= sum over blocks g = 0..ng-1 of part[g][o], in block order
+static bool gram_fits(int S, int M) {
+    const int MS = M * S, nB = S + 3 * MS;
+    const int ntask = S * ((nB + 3) / 4) + MS * ((MS + 3) / 4);  // one thread per 4-output task
+    return S * nB + MS * MS <= GRAM_MAXPER * 256 && ntask <= 256 && gram_smem(S, M) <= 200 * 1024;
+}
+
+// out[o] (+)= sum over blocks g = 0..ng-1 of part[g][o]: one warp per output, lane l summing
+// blocks l, l + 32, ... in order, then a fixed butterfly (the same order on every call)
 __global__ void k_gram_reduce(const double *__restrict__ part, int ng, int nout, int accumulate,
                               double *__restrict__ out) {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    const int o = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (o >= nout) return;
     double s = 0.0;
-    for (int g = 0; g < ng; ++g) s += part[(long long)g * nout + o];
-    out[o] = accumulate ? out[o] + s : s;
+    for (int g = lane; g < ng; g += 32) s += part[(long long)g * nout + o];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) s += __shfl_xor_sync(0xffffffffu, s, d);
+    if (lane == 0) out[o] = accumulate ? out[o] + s : s;
 }
 
 static int smax_of(int p, int64_t nf) {
@@ -346,21 +380,22 @@ static int gram_grid(const nvb_handle *h) {
 }
 
 // G (+)= the Gram matrices of (u, v) on the device, through block partials part[gram_grid *
-// gram_len] (no host synchronisation).
+// gram_len] (no host synchronisation).  G == nullptr: only the block partials are formed
+// (accumulate: added to the partials already there); adjoint_gram_reduce sums them later.
 template <typename T>
 static void gram_launch(nvb_handle *h, const T *u, const T *v, double *G, int accumulate, double *part) {
     const System &sys = h->sys;
     const Plan &pl = h->plan;
     const int S = sys.S, M = sys.M;
-    const int MS = M * S, nA = S + MS, nB = S + 3 * MS;
     const int nout = gram_len(S, M);
     if (!gram_fits(S, M)) fail(NVB_ERR_ARG, "adjoint: too many modes x states for the Gram path");
     const long long Ns = sys.dimen;
     const int grid = gram_grid(h);
-    const size_t shm = (size_t)GRAM_TR * (nA + nB) * sizeof(double);
+    const size_t shm = gram_smem(S, M);
     if (shm > 48 * 1024) CK(cudaFuncSetAttribute(k_adj_gram<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-    k_adj_gram<T><<<grid, 256, shm, h->stream>>>(u, v, pl.d_etab, pl.nmax, pl.d_nfunc, pl.d_shft, M, S, Ns, part);
-    k_gram_reduce<<<(nout + 255) / 256, 256, 0, h->stream>>>(part, grid, nout, accumulate, G);
+    k_adj_gram<T><<<grid, 256, shm, h->stream>>>(u, v, pl.d_etab, pl.nmax, pl.d_nfunc, pl.d_shft, M, S, Ns,
+                                                 G ? 0 : accumulate, part);
+    if (G) k_gram_reduce<<<(nout * 32 + 255) / 256, 256, 0, h->stream>>>(part, grid, nout, accumulate, G);
     CK(cudaGetLastError());
 }
 
@@ -568,6 +603,12 @@ int64_t adjoint_gram_part_len(const nvb_handle *h) { return (int64_t)gram_grid(h
 void adjoint_gram_add(nvb_handle *h, const void *u, const void *v, int dtype, double *G, int accumulate, double *part) {
     if (dtype == NVB_DTYPE_F32) gram_launch<float>(h, (const float *)u, (const float *)v, G, accumulate, part);
     else gram_launch<double>(h, (const double *)u, (const double *)v, G, accumulate, part);
+}
+
+void adjoint_gram_reduce(nvb_handle *h, const double *part, double *G) {
+    const int nout = (int)adjoint_gram_len(h);
+    k_gram_reduce<<<(nout * 32 + 255) / 256, 256, 0, h->stream>>>(part, gram_grid(h), nout, 0, G);
+    CK(cudaGetLastError());
 }
 
 void adjoint_gram_grad(nvb_handle *h, const double *G, double *grad) {

@@ -482,7 +482,7 @@ int nvb_seed_overlap(nvb_handle *h, double *overlap) {
 int nvb_set_checkpoints(nvb_handle *h, int64_t k) {
     return guarded([&] {
         if (!h) fail(NVB_ERR_ARG, "null handle");
-        if (k < 0) fail(NVB_ERR_ARG, "checkpoint interval < 0");
+        if (k < -1) fail(NVB_ERR_ARG, "checkpoint interval < -1");
         ensure_device(h);
         if (k != h->ck_k) ckpt_free(h);
         h->ck_k = k;

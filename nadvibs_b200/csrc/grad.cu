@@ -88,10 +88,11 @@ __global__ void k_replay(T *__restrict__ w, const T *__restrict__ c, const T *__
 }
 
 // rbar = vb_next / beta_i + btot v_{i+1},  btot = bbar_i - <vb_next, v_{i+1}> / beta_i  (bbar_i and
-// the dot product read from device memory)
+// the dot product read from device memory; v_{i+1} = sn * vn)
 __global__ void k_rbar(double *__restrict__ rbar, const double *__restrict__ vbn, const double *__restrict__ vn,
-                       double inv_be, const double *__restrict__ bbar_i, const double *__restrict__ dot1, long long n) {
-    const double btot = *bbar_i - *dot1 * inv_be;
+                       double sn, double inv_be, const double *__restrict__ bbar_i, const double *__restrict__ dot1,
+                       long long n) {
+    const double btot = (*bbar_i - *dot1 * inv_be) * sn;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
         rbar[i] = inv_be * vbn[i] + btot * vn[i];
@@ -119,7 +120,9 @@ __global__ void k_bbar_sub(double *__restrict__ bbar, const double *__restrict__
 struct DevBuf {
     void *p = nullptr;
     DevBuf() = default;
-    explicit DevBuf(size_t bytes) { CK(cudaMalloc(&p, bytes)); }
+    explicit DevBuf(size_t bytes) {
+        if (bytes) CK(cudaMalloc(&p, bytes));
+    }
     ~DevBuf() {
         if (p) cudaFree(p);
     }
@@ -131,7 +134,92 @@ struct DevBuf {
 
 // ---------------------------------------------------------------- checkpoints of the forward
 
+static void rec_free(nvb_handle *h) {
+    if (h->rec_v) cudaFree(h->rec_v);
+    if (h->rec_w) cudaFree(h->rec_w);
+    if (h->rec_vs) cudaFree(h->rec_vs);
+    h->rec_v = h->rec_w = nullptr;
+    h->rec_vs = nullptr;
+    h->rec_cap = h->rec_n = 0;
+    h->rec_ok = false;
+}
+
+// The full record (ck_k = -1) for iterations 1..total_iters, from the seed: kept only when it
+// and the sweep's FP64 work vectors fit the backward budget (nvb_set_backward_memory, default
+// 85 % of the free device memory); otherwise nothing is recorded and the sweep replays.
+static void rec_reserve(nvb_handle *h, int64_t total_iters) {
+    if (h->iters == 0) h->rec_n = 0;
+    if (h->rec_n != h->iters) {  // a record must run contiguously from the seed
+        h->rec_ok = false;
+        return;
+    }
+    if (h->rec_ok && total_iters <= h->rec_cap) return;
+    const size_t per = (size_t)h->ntotal() * h->elem_size(), per64 = (size_t)h->ntotal() * sizeof(double);
+    const size_t keep = h->rec_ok ? (size_t)h->rec_n : 0;
+    size_t freeb = 0, totalb = 0;
+    CK(cudaMemGetInfo(&freeb, &totalb));
+    const double held = h->rec_ok ? (double)(2 * h->rec_cap + 2) * (double)per : 0.0;
+    const double budget = h->grad_budget > 0 ? (double)h->grad_budget : 0.85 * ((double)freeb + held);
+    const double need = (double)(2 * total_iters + 2) * (double)per + 5.0 * (double)per + 10.0 * (double)per64;
+    if (need > budget) {
+        rec_free(h);
+        return;
+    }
+    void *nv = nullptr, *nw = nullptr;
+    double *ns = nullptr;
+    bool ok = cudaMalloc(&nv, (size_t)(total_iters + 2) * per) == cudaSuccess &&
+              cudaMalloc(&nw, (size_t)std::max<int64_t>(total_iters, 1) * per) == cudaSuccess &&
+              cudaMalloc((void **)&ns, (size_t)(total_iters + 2) * sizeof(double)) == cudaSuccess;
+    if (!ok) {
+        (void)cudaGetLastError();  // an out-of-memory return is not sticky: clear it, record nothing
+        if (nv) cudaFree(nv);
+        if (nw) cudaFree(nw);
+        if (ns) cudaFree(ns);
+        rec_free(h);
+        return;
+    }
+    CK(cudaMemsetAsync(nv, 0, per, h->stream));  // v_0 = 0
+    CK(cudaMemsetAsync(ns, 0, sizeof(double), h->stream));
+    if (keep > 0) {
+        CK(cudaMemcpyAsync((char *)nv + per, (char *)h->rec_v + per, (keep + 1) * per, cudaMemcpyDeviceToDevice,
+                           h->stream));
+        CK(cudaMemcpyAsync(nw, h->rec_w, keep * per, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(ns + 1, h->rec_vs + 1, (keep + 1) * sizeof(double), cudaMemcpyDeviceToDevice,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    const int64_t n_keep = (int64_t)keep;
+    rec_free(h);
+    h->rec_v = nv;
+    h->rec_w = nw;
+    h->rec_vs = ns;
+    h->rec_cap = total_iters;
+    h->rec_n = n_keep;
+    h->rec_ok = true;
+}
+
+// At the start of iteration it (buffers cur = v_it with its scale) and after its H.v (work =
+// w_it): the full record's copies.  At the end of a run, v_{it+1}.
+void rec_save_v(nvb_handle *h, int64_t it) {
+    if (h->ck_k != -1 || !h->rec_ok || it > h->rec_cap + 1 || h->rec_n < it - 1) return;
+    const size_t per = (size_t)h->ntotal() * h->elem_size();
+    CK(cudaMemcpyAsync((char *)h->rec_v + (size_t)it * per, h->buf[h->cur], per, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->rec_vs + it, h->d_scale + h->cur, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+}
+
+void rec_save_w(nvb_handle *h, int64_t it) {
+    if (h->ck_k != -1 || !h->rec_ok || it > h->rec_cap || h->rec_n != it - 1) return;
+    const size_t per = (size_t)h->ntotal() * h->elem_size();
+    CK(cudaMemcpyAsync((char *)h->rec_w + (size_t)(it - 1) * per, h->buf[h->work], per, cudaMemcpyDeviceToDevice,
+                       h->stream));
+    h->rec_n = it;
+}
+
 void ckpt_reserve(nvb_handle *h, int64_t total_iters) {
+    if (h->ck_k == -1) {
+        rec_reserve(h, total_iters);
+        return;
+    }
     if (h->ck_k <= 0) return;
     const int64_t need = (total_iters + h->ck_k - 1) / h->ck_k;
     if (need <= h->ck_cap) return;
@@ -175,6 +263,7 @@ void ckpt_free(nvb_handle *h) {
     h->ck_buf = nullptr;
     h->ck_scale = nullptr;
     h->ck_cap = h->ck_count = 0;
+    rec_free(h);
 }
 
 // ---------------------------------------------------------------- replay
@@ -315,25 +404,40 @@ struct Sweep {
         auto V = [&](int64_t j, double *dst) { to64(dst, nat(segv, j - (c - 1)), segs[j - (c - 1)]); };
         for (int64_t i = e; i >= c; --i) {
             const double al = h->alpha[i], be = h->beta[i], bprev = h->beta[i - 1];
-            double *vn = v64[0], *vi = v64[1], *vp = v64[2];
-            V(i + 1, vn);
-            V(i, vi);
-            if (i > 1) V(i - 1, vp);
-            to64(w64, nat(segw, i - c), 1.0);  // w_i = H v_i from the replay
-            device_dot_async(h, vb_next, 1.0, vn, 1.0, NVB_DTYPE_F64, d_dots);
-            k_rbar<<<g, 256, 0, h->stream>>>(rbar, vb_next, vn, 1.0 / be, d_bbar + i, d_dots, N);
+            // v_{i+1}, v_{i-1} and w_i are read where they are stored (FP64 handles: the stored
+            // vector and its scale, no copy); v_i, which the adjoint contraction also reads,
+            // and everything of a mixed handle are widened to FP64 first
+            const double *vn = v64[0], *vp = v64[2], *wi = w64, *vi = v64[1];
+            double sn = 1.0, sp = 1.0;
+            if (mixed) {
+                V(i + 1, v64[0]);
+                if (i > 1) V(i - 1, v64[2]);
+                to64(w64, nat(segw, i - c), 1.0);  // w_i = H v_i from the replay
+            } else {
+                vn = (const double *)nat(segv, i + 1 - (c - 1));
+                sn = segs[i + 1 - (c - 1)];
+                if (i > 1) {
+                    vp = (const double *)nat(segv, i - 1 - (c - 1));
+                    sp = segs[i - 1 - (c - 1)];
+                }
+                wi = (const double *)nat(segw, i - c);
+            }
+            V(i, v64[1]);
+            device_dot_async(h, vb_next, 1.0, vn, sn, NVB_DTYPE_F64, d_dots);
+            k_rbar<<<g, 256, 0, h->stream>>>(rbar, vb_next, vn, sn, 1.0 / be, d_bbar + i, d_dots, N);
             device_dot_async(h, rbar, 1.0, vi, 1.0, NVB_DTYPE_F64, d_dots + 1);
             if (i > 1) {
-                device_dot_async(h, rbar, 1.0, vp, 1.0, NVB_DTYPE_F64, d_dots + 2);
+                device_dot_async(h, rbar, 1.0, vp, sp, NVB_DTYPE_F64, d_dots + 2);
                 k_bbar_sub<<<1, 1, 0, h->stream>>>(d_bbar + i - 1, d_dots + 2);
             }
-            k_step<<<g, 256, 0, h->stream>>>(vb_cur, wbar, vb_prev, rbar, w64, vi, al, abar[i - 1], d_dots + 1, bprev,
+            k_step<<<g, 256, 0, h->stream>>>(vb_cur, wbar, vb_prev, rbar, wi, vi, al, abar[i - 1], d_dots + 1, bprev,
                                              i > 1 ? 1 : 0, N);
             hv_any(h, wbar, wv, NVB_DTYPE_F64, nullptr, nullptr, nullptr);  // H wbar
             k_lin<<<g, 256, 0, h->stream>>>(vb_cur, 1.0, wv, 0.0, nullptr, 1, N);
             CK(cudaGetLastError());
             if (G) {
-                adjoint_gram_add(h, wbar, vi, NVB_DTYPE_F64, G, gram_started ? 1 : 0, gpart);
+                // per-block partials summed over the sweep; one reduction at the end
+                adjoint_gram_add(h, wbar, vi, NVB_DTYPE_F64, nullptr, gram_started ? 1 : 0, gpart);
                 gram_started = true;
             } else {
                 hv_adjoint(h, wbar, vi, NVB_DTYPE_F64, gstep.data());
@@ -420,7 +524,10 @@ static bool plan_levels(int64_t n, double vectors, int64_t *L, int64_t *B, int64
 void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const double *bbar_in, int64_t k,
                       double *grad) {
     if (n < 1 || n > h->iters) fail(NVB_ERR_ARG, "n must be in 1..iterations done");
-    if (k < 0) fail(NVB_ERR_ARG, "checkpoint interval must be >= 0 (0 = automatic from the memory budget)");
+    if (k < -1) fail(NVB_ERR_ARG, "checkpoint interval must be >= -1 (0 = automatic, -1 = the forward's full record)");
+    // the forward's full record, when it was kept and covers n: nothing is replayed
+    const bool from_record = k == -1 && h->ck_k == -1 && h->rec_ok && h->rec_n >= n;
+    if (k == -1 && !from_record) k = 0;  // no record (it did not fit): the automatic plan
     if (h->reorthog > 0) fail(NVB_ERR_STATE, "the reverse sweep differentiates plain Lanczos (reorthog = 0)");
     if (!(h->beta[n] > 0.0)) fail(NVB_ERR_STATE, "beta_n is zero: v_{n+1} does not exist");
     {
@@ -445,7 +552,10 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
     // one replay from the seed) and bmax = k.  k = 0 picks the shallowest recursion that fits the
     // memory budget, over the forward's pairs when they were recorded, else from the seed.
     int64_t top = 0;  // interval of the top-level pairs in h->ck_buf, 0 = start from the seed pair
-    if (k > 0) {
+    if (from_record) {
+        W.B = 1;
+        W.bmax = n;
+    } else if (k > 0) {
         W.bmax = std::min(k, n);
         W.B = (n + W.bmax - 1) / W.bmax;  // ranges of the one level
         top = n > k ? k : 0;
@@ -468,8 +578,10 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
     h->bw_plan[0] = top;
     h->bw_plan[1] = W.B;
     h->bw_plan[2] = W.bmax;
-    // base storage and work vectors
-    DevBuf segv((size_t)(W.bmax + 2) * W.per), segw((size_t)(W.bmax + 1) * W.per), b0(W.per), b1(W.per), b2(W.per);
+    // base storage and work vectors (no base storage when the forward's record is the base range)
+    const size_t nbase = from_record ? 0 : 1;
+    DevBuf segv(nbase * (size_t)(W.bmax + 2) * W.per), segw(nbase * (size_t)(W.bmax + 1) * W.per),
+        b0(nbase * W.per), b1(nbase * W.per), b2(nbase * W.per);
     DevBuf vbn(W.per64), vbc(W.per64), vbp(W.per64), rb(W.per64), wb(W.per64), wvb(W.per64), c0(W.per64),
         c1(W.per64), c2(W.per64), cw(W.per64);
     W.segv = segv.p;
@@ -503,11 +615,21 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
     if (glen > 0) {
         W.G = (double *)gbuf.p;
         W.gpart = W.G + glen;
+        CK(cudaMemsetAsync(W.gpart, 0, (size_t)gplen * sizeof(double), h->stream));
     }
     W.grad = grad;
     std::fill(grad, grad + W.nc, 0.0);
     W.gstep.assign(W.nc, 0.0);
-    if (top == 0) {
+    if (from_record) {
+        // the base range 1..n straight from the record: v_j in slot j, w_j in slot j - 1
+        W.segv = h->rec_v;
+        W.segw = h->rec_w;
+        CK(cudaMemcpyAsync(W.segs.data(), h->rec_vs, (size_t)(n + 2) * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        W.segs[0] = 0.0;
+        W.reverse_steps(1, n);
+    } else if (top == 0) {
         // from the seed pair (v_0 = 0, v_1 = the seed)
         DevBuf zero(W.per), seed(W.per);
         CK(cudaMemsetAsync(zero.p, 0, W.per, h->stream));
@@ -523,7 +645,10 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
             W.reverse_range(P, 1 + s2 * top, std::min((s2 + 1) * top, n));
         }
     }
-    if (W.G) adjoint_gram_grad(h, W.G, grad);  // the gradient of the summed Gram matrices
+    if (W.G) {
+        adjoint_gram_reduce(h, W.gpart, W.G);  // the Gram matrices summed over all steps
+        adjoint_gram_grad(h, W.G, grad);       // and the gradient they give (linear in them)
+    }
     CK(cudaStreamSynchronize(h->stream));
     h->bw_plan[3] = W.replayed;
     check_kernel_flags(h);

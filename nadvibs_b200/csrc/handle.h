@@ -52,6 +52,13 @@ struct nvb_handle {
     int64_t ck_k = 0, ck_count = 0, ck_cap = 0;
     void *ck_buf = nullptr;
     double *ck_scale = nullptr;
+    // full record of the forward (ck_k = -1), when it fits the backward budget: v_0 = 0,
+    // v_1..v_{n+1} in native precision with their scales, and w_j = H v_j (j = 1..n), so that
+    // the reverse sweep replays nothing
+    void *rec_v = nullptr, *rec_w = nullptr;
+    double *rec_vs = nullptr;
+    int64_t rec_cap = 0, rec_n = 0;
+    bool rec_ok = false;
     // the reverse sweep: device-memory budget for k = 0 (bytes, 0 = 85% of free memory) and
     // the last sweep's plan (top-level interval, branching, longest stored range, replayed H.v)
     int64_t grad_budget = 0;
@@ -93,6 +100,8 @@ void hv_adjoint(nvb_handle *h, const void *u, const void *v, int dtype, double *
 int64_t adjoint_gram_len(const nvb_handle *h);
 int64_t adjoint_gram_part_len(const nvb_handle *h);
 void adjoint_gram_add(nvb_handle *h, const void *u, const void *v, int dtype, double *G, int accumulate, double *part);
+// G = sum over blocks of the partials that adjoint_gram_add(..., G = nullptr, ...) accumulated
+void adjoint_gram_reduce(nvb_handle *h, const double *part, double *G);
 void adjoint_gram_grad(nvb_handle *h, const double *G, double *grad);
 void hellmann_feynman(nvb_handle *h, int64_t nroots, double *grad, double *energies);
 void displaced_seed(nvb_handle *h);
@@ -100,6 +109,8 @@ double seed_fill(nvb_handle *h, void *buf, const std::vector<double> &w);
 std::vector<double> seed_weights(const nvb_handle *h);
 void ckpt_reserve(nvb_handle *h, int64_t total_iters);
 void ckpt_save(nvb_handle *h, int64_t it);
+void rec_save_v(nvb_handle *h, int64_t it);  // the full record (checkpoint interval -1)
+void rec_save_w(nvb_handle *h, int64_t it);
 void ckpt_free(nvb_handle *h);
 void lanczos_backward(nvb_handle *h, int64_t n, const double *abar, const double *bbar, int64_t k, double *grad);
 int64_t ncoef_of(const nvb_handle *h);

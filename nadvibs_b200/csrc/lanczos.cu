@@ -363,9 +363,11 @@ static void lanczos_iter(nvb_handle *h, int64_t it, int slot) {
     const int dt = h->precision == NVB_MIXED ? NVB_DTYPE_F32 : NVB_DTYPE_F64;
     int nb = 0;
     ckpt_save(h, it);
+    rec_save_v(h, it);
     archive_push(h, it);
     if (h->timing) CK(cudaEventRecord(h->ev[3 * slot], h->stream));
     hv_any(h, h->buf[h->cur], h->buf[h->work], dt, h->d_scale + h->cur, h->d_part, &nb);
+    rec_save_w(h, it);  // w_it = H v_it, before pass B turns it into the residual
     if (h->timing) CK(cudaEventRecord(h->ev[3 * slot + 1], h->stream));
     k_finalize<<<1, FIN_THREADS, 0, h->stream>>>(h->d_part, nb, h->d_alpha + it, 0, nullptr, h->d_status, (int)it);
     if (dt == NVB_DTYPE_F32) passB_launch<float>(h, it, &nb);
@@ -475,6 +477,7 @@ void lanczos_run(nvb_handle *h, int64_t niter) {
         }
     }
     h->iters += niter;
+    rec_save_v(h, h->iters + 1);  // v_{n+1} of the full record
     h->alpha.resize(h->iters + 1);
     h->beta.resize(h->iters + 1);
     if (h->iters > 0) {

@@ -9,8 +9,8 @@ torch = pytest.importorskip("torch")
 
 from nadvibs_b200 import _lib as L
 from nadvibs_b200 import synth
-from nadvibs_b200.autograd import (convolved_spectrum, ritz, split_theta, tridiag_eig_backward,
-                                   tridiag_eigh)
+from nadvibs_b200.autograd import (converged_mask, converged_spectrum, convolved_spectrum, ritz, split_theta,
+                                   tridiag_eig_backward, tridiag_eigh)
 
 pytestmark = pytest.mark.gpu
 
@@ -258,6 +258,44 @@ def _config4():
     return p, np.concatenate([synth.flatten_pot(pot), cc, om])
 
 
+@pytest.mark.parametrize("prec", [L.NVB_FP64, L.NVB_MIXED])
+def test_full_forward_record_matches_replayed_plans(prec):
+    """Checkpoint interval -1: the forward records every v_j and H v_j, the reverse sweep replays
+    nothing, and the gradient equals the automatic (replaying) plan's and one level of interval
+    7 to 1e-12 relative.  A budget too small for the record leaves it out and the same call
+    falls back to the automatic plan."""
+    p, theta = _system(21, 2, [4, 3, 4, 3], 2)
+    n = 40
+    rng = np.random.default_rng(8)
+    gE = rng.normal(size=n)
+    gI = rng.normal(size=n)
+    g_auto = _gradient(p, theta, n, gE, gI, 0, record=False, precision=prec)
+    g_k7 = _gradient(p, theta, n, gE, gI, 7, precision=prec)
+    pot, cc, om = split_theta(theta, p.nstates, p.nmodes)
+    with L.Handle.from_arrays(p, om, cc, pot, precision=prec) as h:
+        h.set_checkpoints(-1)
+        h.seed()
+        a, b = h.lanczos(n)
+        E, S = tridiag_eigh(a[:n], b[1:n])
+        abar, bbar_off = tridiag_eig_backward(E, S, gE, gI)
+        bbar = np.zeros(n)
+        bbar[: n - 1] = bbar_off
+        g_rec = h.lanczos_backward(n, abar, bbar, -1)
+        assert h.backward_plan()["replayed_hv"] == 0
+    scale = np.abs(g_auto).max()
+    assert np.abs(g_rec - g_auto).max() <= 1e-12 * scale
+    assert np.abs(g_rec - g_k7).max() <= 1e-12 * scale
+    with L.Handle.from_arrays(p, om, cc, pot, precision=prec) as h:
+        h.set_backward_memory(1)  # nothing fits: no record, and the sweep must then replay
+        h.set_checkpoints(-1)
+        h.seed()
+        h.lanczos(n)
+        h.set_backward_memory(0)
+        g_fb = h.lanczos_backward(n, abar, bbar, -1)
+        assert h.backward_plan()["replayed_hv"] > 0
+    assert np.abs(g_fb - g_auto).max() <= 1e-12 * scale
+
+
 def test_config4_converged_roots_match_hellmann_feynman():
     """Gradient system (2 states, basis [14,12,10,8,8,6], 400 iterations, checkpoints every 50):
     the reverse sweep for a random combination of the converged roots among the lowest 20
@@ -286,6 +324,40 @@ def test_config4_converged_roots_match_hellmann_feynman():
         _, ghf = h.hellmann_feynman(20)
     ref = c @ ghf
     assert np.abs(g - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_config4_converged_spectrum_gradient_meets_1e5_against_finite_differences():
+    """Gradient system (2 states, basis [14,12,10,8,8,6], 400 plain iterations, automatic
+    checkpoint plan): the Gaussian-convolved spectrum (sigma 20 cm^-1, 2048 points) of the
+    converged Ritz values (bji < 1e-9 hartree in the unperturbed run, ghost copies included,
+    the mask kept fixed) against central differences with h = 1e-3 cm^-1 on expansion
+    coefficients, block constants and frequencies: 1e-5 relative to max |fd|."""
+    p, theta = _config4()
+    n = 400
+    grid = torch.linspace(-200.0, 8000.0, 2048, dtype=torch.float64)
+    w = torch.from_numpy(np.random.default_rng(4).normal(size=2048))
+    th = torch.from_numpy(theta.copy()).requires_grad_(True)
+    E, I, bji = ritz(th, p, n, residuals=True)
+    mask = converged_mask(bji, 1e-9)
+    assert int(mask.sum()) >= 10
+    (w * converged_spectrum(E, I, mask, grid, 20.0)).sum().backward()
+    g = th.grad.numpy()
+    npot = theta.size - 3 - p.nmodes
+
+    def f(x):
+        E2, I2 = _forward(p, x, n)
+        return float((w * converged_spectrum(torch.from_numpy(E2), torch.from_numpy(I2), mask, grid, 20.0)).sum())
+
+    idx = [0, 3, 10, 40, 77, npot, npot + 2, theta.size - 1, theta.size - 4]
+    fd = []
+    for i in idx:
+        hs = 1e-3 / 219474.6313705 * (0.05 if i < npot else 1.0)
+        tp, tm = theta.copy(), theta.copy()
+        tp[i] += hs
+        tm[i] -= hs
+        fd.append((f(tp) - f(tm)) / (2 * hs))
+    fd = np.array(fd)
+    assert np.abs(g[idx] - fd).max() <= 1e-5 * np.abs(fd).max()
 
 
 def test_config4_spectrum_gradient_against_finite_differences():
