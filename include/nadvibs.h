@@ -153,10 +153,37 @@ int nvb_lanczos(nvb_handle *h, int64_t niter, double *alpha, double *beta);
 /* Re-orthogonalisation mode as in basis.in (Source/secondary.f90:847-848): reorthog 0 none,
  * 1 omega recurrence with exact checks every chkorthog iterations, 2 exact overlaps;
  * partial re-orthogonalisation (set_omega + partial_orthog, Source/top.f90:844-1005) runs after
- * every iteration from the second.  It needs every Lanczos vector in the device archive
- * (options archive_max >= total iterations), else nvb_lanczos fails with NVB_ERR_ARG.  The
+ * every iteration from the second.  It needs every Lanczos vector in the archive (options
+ * archive_max, or nvb_set_archive, >= total iterations), else nvb_lanczos fails with
+ * NVB_ERR_ARG.  The
  * omega recurrence's random draws use the options' seed (the reference is unseeded). */
 int nvb_set_reorthog(nvb_handle *h, int64_t reorthog, int64_t chkorthog);
+
+/* Where the archive of Lanczos vectors lives, from the next nvb_seed on (the reference's disk
+ * archive nadvibs.34.<rank>, Source/top.f90:570-571,595-598, written and read by write_ga /
+ * read_ga, Source/secondary.f90:273-308): kind 0 device memory (the same as the options'
+ * archive_max = max_vectors), 1 pinned host memory (allocated in blocks as the run grows), 2
+ * the file at path in the reference's layout (each vector as nstates records of dimen FP64
+ * values, vector after vector, whatever the handle's precision).  Host memory and the file are
+ * streamed to the device in chunks of whole vectors for re-orthogonalisation and Ritz vectors.
+ * With a file archive that holds every earlier vector, re-orthogonalisation resumes after
+ * nvb_load_restart. */
+int nvb_set_archive(nvb_handle *h, int64_t kind, int64_t max_vectors, const char *path);
+
+/* The intervals of Lanczos vectors that partial re-orthogonalisation (partial_orthog,
+ * Source/top.f90:910-1005) orthogonalised against since the seed, in order: entry i =
+ * (iteration[i], lo[i], hi[i]), 1-based, at most max_entries written (arrays may be NULL);
+ * *count = the number of entries.  No reference counterpart (the reference does not report
+ * them). */
+int nvb_reorth_log(nvb_handle *h, int64_t max_entries, int64_t *iteration, int64_t *lo, int64_t *hi,
+                   int64_t *count);
+
+/* The orthogonality estimates of re-orthogonalisation (set_omega, Source/top.f90:844-908),
+ * entries 0..n: omega1 = omega(1,:) and omega2 = omega(2,:) as they stand (the reference writes
+ * both to restart.log), omega2_step = omega(2,:) of the last iteration as partial_orthog saw
+ * it, before the resets of the orthogonalised intervals.  Arrays may be NULL.  No reference
+ * counterpart as an entry point. */
+int nvb_reorth_omega(nvb_handle *h, int64_t n, double *omega1, double *omega2, double *omega2_step);
 
 /* Ritz system of T_n, n <= iters (compute_ritzsystem, Source/secondary.f90:240-257):
  * E[n] ascending (hartree), bji[n] = |beta(n) s(n,i)|, inten[n] = s(1,i)^2, sign[n] of

@@ -53,6 +53,9 @@ _SIGS = {
     "nvb_get_sizes": [C.c_void_p] + [C.c_void_p] * 6,
     "nvb_hv_kernel_in_use": [C.c_void_p, C.c_int64, C.c_void_p],
     "nvb_set_checkpoints": [C.c_void_p, C.c_int64],
+    "nvb_set_archive": [C.c_void_p, C.c_int64, C.c_int64, C.c_char_p],
+    "nvb_reorth_log": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "nvb_reorth_omega": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_set_fault_test": [C.c_void_p, C.c_int64],
     "nvb_set_displaced_seed": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_seed_overlap": [C.c_void_p, C.c_void_p],
@@ -306,6 +309,27 @@ class Handle:
 
     def set_reorthog(self, reorthog: int, chkorthog: int = 100):
         check(lib().nvb_set_reorthog(self.ptr, reorthog, chkorthog))
+
+    ARCHIVE_DEVICE, ARCHIVE_HOST, ARCHIVE_FILE = 0, 1, 2
+
+    def set_archive(self, kind: int, max_vectors: int, path: str | None = None):
+        """Where the Lanczos-vector archive lives from the next seed (nvb_set_archive): 0 device
+        memory, 1 pinned host memory, 2 a file at path in the reference's nadvibs.34 layout."""
+        check(lib().nvb_set_archive(self.ptr, kind, max_vectors, path.encode() if path else None))
+
+    def reorth_omega(self, n: int):
+        """(omega1[0..n], omega2[0..n], omega2 of the last step before its resets) (nvb_reorth_omega)."""
+        w1, w2, w3 = (np.zeros(n + 1) for _ in range(3))
+        check(lib().nvb_reorth_omega(self.ptr, n, _p(w1), _p(w2), _p(w3)))
+        return w1, w2, w3
+
+    def reorth_log(self) -> np.ndarray:
+        """(iteration, lo, hi) of every interval partial re-orthogonalisation used (nvb_reorth_log)."""
+        n = C.c_int64()
+        check(lib().nvb_reorth_log(self.ptr, 0, None, None, None, C.byref(n)))
+        it, lo, hi = (np.zeros(max(n.value, 1), dtype=np.int64) for _ in range(3))
+        check(lib().nvb_reorth_log(self.ptr, n.value, _p(it), _p(lo), _p(hi), C.byref(n)))
+        return np.stack([it[:n.value], lo[:n.value], hi[:n.value]], axis=1)
 
     def ncoef(self) -> int:
         sz = self.sizes()

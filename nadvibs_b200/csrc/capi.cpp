@@ -252,7 +252,13 @@ int nvb_set_precision(nvb_handle *h, int64_t precision) {
             CKA(cudaStreamSynchronize(h->stream));
             for (int i = 0; i < 3; ++i)
                 if (h->buf[i]) { cudaFree(h->buf[i]); h->buf[i] = nullptr; }
-            if (h->arch) { cudaFree(h->arch); h->arch = nullptr; h->arch_cap = h->arch_n = 0; }
+            {
+                const int kind = h->arch_kind;
+                const int64_t cap = archive_capacity(h);
+                const std::string path = h->arch_path;
+                archive_free(h);  // the archive's vectors are in the old precision: start afresh
+                archive_configure(h, kind, cap, path.c_str());
+            }
             h->precision = (int)precision;
         }
         h->seeded = false;
@@ -418,6 +424,40 @@ int nvb_lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *sta
         if (!h) fail(NVB_ERR_ARG, "null handle");
         ensure_device(h);
         lead_contributors(h, nroots, k, state, index, c2, phase, pct, rootinfo_path);
+    });
+}
+
+int nvb_set_archive(nvb_handle *h, int64_t kind, int64_t max_vectors, const char *path) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        ensure_device(h);
+        if (h->stream) CKA(cudaStreamSynchronize(h->stream));
+        archive_configure(h, (int)kind, max_vectors, path);  // filled from the next nvb_seed on
+    });
+}
+
+int nvb_reorth_log(nvb_handle *h, int64_t max_entries, int64_t *iteration, int64_t *lo, int64_t *hi, int64_t *count) {
+    return guarded([&] {
+        if (!h || !count) fail(NVB_ERR_ARG, "null argument");
+        const int64_t n = (int64_t)h->orth_log.size();
+        *count = n;
+        for (int64_t i = 0; i < std::min(n, max_entries); ++i) {
+            if (iteration) iteration[i] = h->orth_log[(size_t)i][0];
+            if (lo) lo[i] = h->orth_log[(size_t)i][1];
+            if (hi) hi[i] = h->orth_log[(size_t)i][2];
+        }
+    });
+}
+
+int nvb_reorth_omega(nvb_handle *h, int64_t n, double *omega1, double *omega2, double *omega2_step) {
+    return guarded([&] {
+        if (!h) fail(NVB_ERR_ARG, "null handle");
+        if (n < 0) fail(NVB_ERR_ARG, "n < 0");
+        for (int64_t i = 0; i <= n; ++i) {
+            if (omega1) omega1[i] = i < (int64_t)h->omega1.size() ? h->omega1[(size_t)i] : 0.0;
+            if (omega2) omega2[i] = i < (int64_t)h->omega2.size() ? h->omega2[(size_t)i] : 0.0;
+            if (omega2_step) omega2_step[i] = i < (int64_t)h->omega_pre.size() ? h->omega_pre[(size_t)i] : 0.0;
+        }
     });
 }
 

@@ -2,7 +2,11 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
+#include <cstdio>
+#include <functional>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "plan.h"
@@ -33,14 +37,27 @@ struct nvb_handle {
     double *d_part = nullptr;   // reduction partials
     int64_t part_len = 0;
     std::vector<double> alpha, beta;  // host copies: alpha[1..iters] (alpha[0] unused), beta[0..iters]
-    // archive of normalised Lanczos vectors v_1..v_k (device, precision of the handle)
+    // archive of normalised Lanczos vectors v_1..v_k (archive.cu): device memory (arch, the
+    // handle's precision), pinned host blocks, or a file in the reference's FP64 layout
+    int arch_kind = 0;  // ARCH_DEVICE, ARCH_HOST, ARCH_FILE
     void *arch = nullptr;
     int64_t arch_cap = 0, arch_n = 0;
+    int64_t harch_max = 0;              // capacity of the host kinds (vectors)
+    std::vector<void *> harch_blocks;   // pinned blocks of whole vectors (ARCH_HOST)
+    std::string arch_path;              // ARCH_FILE
+    FILE *arch_file = nullptr;
+    void *arch_stage[2] = {nullptr, nullptr};  // device staging ring of the streamed chunks
+    void *arch_stage64 = nullptr;              // FP64 staging of the file's records
+    void *arch_bounce = nullptr;               // pinned bounce buffer of the file
+    cudaStream_t arch_stream = nullptr;        // copy stream of the staging ring
+    cudaEvent_t arch_ready[2] = {nullptr, nullptr}, arch_free[2] = {nullptr, nullptr};
     // re-orthogonalisation
     int64_t reorthog = 0, chkorthog = 100;
     std::vector<double> omega1, omega2;  // omega(1,0:n), omega(2,0:n)
     bool firststep = true;
     std::vector<std::pair<int64_t, int64_t>> orth_ranges;
+    std::vector<std::array<int64_t, 3>> orth_log;  // (iteration, lo, hi) of every Gram-Schmidt interval
+    std::vector<double> omega_pre;                 // omega(2, 0:it) of the last step, before its resets
     uint64_t rng_state = 0;
     // per-phase device timing (CUDA events on the handle's stream)
     bool timing = false;
@@ -90,8 +107,17 @@ double device_dot(nvb_handle *h, const void *a, double sa, const void *b, double
 void device_dot_async(nvb_handle *h, const void *a, double sa, const void *b, double sb, int dtype, double *out_dev);
 void *scratch_vector(nvb_handle *h, size_t bytes);
 void grow_scalars_public(nvb_handle *h, int64_t need);
+constexpr int ARCH_DEVICE = 0, ARCH_HOST = 1, ARCH_FILE = 2;
+void archive_configure(nvb_handle *h, int kind, int64_t max_vectors, const char *path);
+int64_t archive_capacity(const nvb_handle *h);
+bool archive_holds(const nvb_handle *h, int64_t n);
+void archive_free(nvb_handle *h);
 void archive_ensure(nvb_handle *h, int64_t need);
 void archive_push(nvb_handle *h, int64_t it);
+// fn(base, first, count) over chunks of archive entries lo..hi (1-based), base = the device
+// address of entry `first` (native precision) for kernels on the handle's stream
+void archive_for_chunks(nvb_handle *h, int64_t lo, int64_t hi,
+                        const std::function<void(const void *, int64_t, int64_t)> &fn);
 void save_restart(nvb_handle *h, const char *dir, const char *vdir);
 void load_restart(nvb_handle *h, const char *dir, const char *vdir);
 void hv_adjoint(nvb_handle *h, const void *u, const void *v, int dtype, double *grad);

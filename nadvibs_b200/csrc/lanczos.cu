@@ -234,13 +234,12 @@ void lanczos_free(nvb_handle *h) {
     if (h->d_scale) cudaFree(h->d_scale);
     if (h->d_status) cudaFree(h->d_status);
     if (h->d_part) cudaFree(h->d_part);
-    if (h->arch) cudaFree(h->arch);
+    archive_free(h);
     if (h->tmp) cudaFree(h->tmp);
     h->d_alpha = h->d_beta = h->d_scale = h->d_part = nullptr;
     h->d_status = nullptr;
-    h->arch = h->tmp = nullptr;
+    h->tmp = nullptr;
     h->cap = h->part_len = 0;
-    h->arch_cap = h->arch_n = 0;
     h->tmp_bytes = 0;
 }
 
@@ -430,12 +429,13 @@ void lanczos_run(nvb_handle *h, int64_t niter) {
     archive_ensure(h, h->iters + niter);
     ckpt_reserve(h, h->iters + niter);
     if (h->reorthog > 0) {
-        if (h->opt.archive_max < h->iters + niter)
-            fail(NVB_ERR_ARG, "re-orthogonalisation needs every Lanczos vector: set archive_max >= " +
-                                  std::to_string(h->iters + niter) + " (the archive lives in device memory)");
+        if (archive_capacity(h) < h->iters + niter)
+            fail(NVB_ERR_ARG, "re-orthogonalisation needs every Lanczos vector: give the archive room for >= " +
+                                  std::to_string(h->iters + niter) +
+                                  " vectors (options archive_max for device memory, or nvb_set_archive)");
         if (h->arch_n != h->iters)
-            fail(NVB_ERR_STATE, "re-orthogonalisation cannot resume from a restart: the earlier Lanczos vectors "
-                                "(the reference's disk archive) are not kept");
+            fail(NVB_ERR_STATE, "re-orthogonalisation cannot resume: the archive does not hold the earlier Lanczos "
+                                "vectors (after a restart only a file archive with every earlier vector does)");
         reorth_run(h, niter);
         return;
     }

@@ -10,7 +10,8 @@
 //    the next step, and beta(n) recomputed.
 // The random draws (gauss_random, Source/function.f90:260-267) come from a seeded generator
 // (the reference's random_seed() is unseeded).  The host keeps omega; overlaps and updates run
-// on the device against the archive, which must hold every Lanczos vector.
+// on the device against the archive (archive.cu: device memory, or pinned host memory / a file
+// streamed to the device in chunks), which must hold every Lanczos vector.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -110,48 +111,67 @@ static double gauss(nvb_handle *h, double mean, double sigma) {
     return mean + sigma * std::sqrt(-2.0 * std::log(r1)) * std::cos(6.283185307179586 * r2);
 }
 
-// overlaps <s*q, v_j> for j in [lo, hi] (1-based archive indices), host result
+// overlaps <s*q, v_j> for j in [lo, hi] (1-based archive indices), host result.  The archive
+// is read chunk by chunk (streamed from the host or the file for those kinds); the block
+// partials of every vector stay on the device until one copy at the end.
 static std::vector<double> overlaps(nvb_handle *h, const void *q, double sq, int64_t lo, int64_t hi) {
+    std::vector<double> out;
+    if (hi < lo) return out;
     const long long n = h->ntotal();
     const int g = md_grid(n);
-    std::vector<double> out;
-    for (int64_t first = lo; first <= hi; first += MD_MAXV) {
-        const int nv = (int)std::min<int64_t>(MD_MAXV, hi - first + 1);
-        ensure_partials(h, (int64_t)g * nv);
-        if (h->precision == NVB_MIXED)
-            k_multi_dot<float><<<g, MD_THREADS, 0, h->stream>>>((const float *)q, sq, (const float *)h->arch, first - 1,
-                                                                nv, n, h->d_part);
-        else
-            k_multi_dot<double><<<g, MD_THREADS, 0, h->stream>>>((const double *)q, sq, (const double *)h->arch,
-                                                                 first - 1, nv, n, h->d_part);
-        CK(cudaGetLastError());
-        std::vector<double> part((size_t)g * nv);
-        CK(cudaMemcpyAsync(part.data(), h->d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        for (int j = 0; j < nv; ++j) {
-            double s = 0.0;
-            for (int b = 0; b < g; ++b) s += part[(size_t)b * nv + j];
-            out.push_back(s);
+    const int64_t cnt = hi - lo + 1;
+    ensure_partials(h, (int64_t)g * cnt);
+    std::vector<std::pair<int64_t, int>> groups;  // (offset from lo, vectors) of each kernel call
+    archive_for_chunks(h, lo, hi, [&](const void *base, int64_t first, int64_t count) {
+        for (int64_t off = 0; off < count; off += MD_MAXV) {
+            const int nv = (int)std::min<int64_t>(MD_MAXV, count - off);
+            const int64_t o = first - lo + off;
+            double *part = h->d_part + (size_t)o * g;
+            if (h->precision == NVB_MIXED)
+                k_multi_dot<float><<<g, MD_THREADS, 0, h->stream>>>((const float *)q, sq, (const float *)base, off, nv,
+                                                                    n, part);
+            else
+                k_multi_dot<double><<<g, MD_THREADS, 0, h->stream>>>((const double *)q, sq, (const double *)base, off,
+                                                                     nv, n, part);
+            CK(cudaGetLastError());
+            groups.push_back({o, nv});
+        }
+    });
+    std::vector<double> part((size_t)g * cnt);
+    CK(cudaMemcpyAsync(part.data(), h->d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    out.assign(cnt, 0.0);
+    for (auto &gr : groups) {
+        const double *pp = part.data() + (size_t)gr.first * g;
+        for (int jv = 0; jv < gr.second; ++jv) {
+            double acc = 0.0;
+            for (int b = 0; b < g; ++b) acc += pp[(size_t)b * gr.second + jv];
+            out[gr.first + jv] = acc;
         }
     }
     return out;
 }
 
+// q -= sum_j c_j v_{lo+j}, the archive read chunk by chunk
 static void subtract(nvb_handle *h, void *q, int64_t lo, const std::vector<double> &c) {
+    if (c.empty()) return;
     const long long n = h->ntotal();
     ensure_partials(h, (int64_t)c.size());
     double *dc = h->d_part;  // the coefficients ride in the reduction scratch (not in use here)
     CK(cudaMemcpyAsync(dc, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    for (size_t off = 0; off < c.size(); off += MD_MAXV) {
-        const int nv = (int)std::min<size_t>(MD_MAXV, c.size() - off);
-        if (h->precision == NVB_MIXED)
-            k_multi_axpy<float><<<md_grid(n), MD_THREADS, 0, h->stream>>>((float *)q, (const float *)h->arch,
-                                                                           lo - 1 + (long long)off, nv, dc + off, n);
-        else
-            k_multi_axpy<double><<<md_grid(n), MD_THREADS, 0, h->stream>>>((double *)q, (const double *)h->arch,
-                                                                            lo - 1 + (long long)off, nv, dc + off, n);
-        CK(cudaGetLastError());
-    }
+    archive_for_chunks(h, lo, lo + (int64_t)c.size() - 1, [&](const void *base, int64_t first, int64_t count) {
+        for (int64_t off = 0; off < count; off += MD_MAXV) {
+            const int nv = (int)std::min<int64_t>(MD_MAXV, count - off);
+            const double *cc = dc + (first - lo) + off;
+            if (h->precision == NVB_MIXED)
+                k_multi_axpy<float><<<md_grid(n), MD_THREADS, 0, h->stream>>>((float *)q, (const float *)base, off, nv,
+                                                                               cc, n);
+            else
+                k_multi_axpy<double><<<md_grid(n), MD_THREADS, 0, h->stream>>>((double *)q, (const double *)base, off,
+                                                                                nv, cc, n);
+            CK(cudaGetLastError());
+        }
+    });
     CK(cudaStreamSynchronize(h->stream));
 }
 
@@ -192,6 +212,7 @@ void reorth_init(nvb_handle *h, int64_t niter_total) {
     if (niter_total + 2 > 2) h->omega2[2] = 1.0;
     h->firststep = true;
     h->orth_ranges.clear();
+    h->orth_log.clear();
 }
 
 // Called after iteration `it` (>= 2) when reorthog > 0.  State: buf[cur] = r_it (raw),
@@ -232,6 +253,7 @@ void reorth_after_iter(nvb_handle *h, int64_t it, int64_t niter_total) {
             }
         }
     }
+    h->omega_pre.assign(w2.begin(), w2.begin() + it + 1);
     // ---- partial_orthog
     if (h->firststep) {
         std::vector<int64_t> oi;
@@ -266,6 +288,7 @@ void reorth_after_iter(nvb_handle *h, int64_t it, int64_t niter_total) {
         std::vector<std::vector<double>> dots;
         for (auto &pr : h->orth_ranges) dots.push_back(overlaps(h, r, 1.0, pr.first, pr.second));
         for (size_t i = 0; i < h->orth_ranges.size(); ++i) {
+            h->orth_log.push_back({it, h->orth_ranges[i].first, h->orth_ranges[i].second});
             subtract(h, r, h->orth_ranges[i].first, dots[i]);
             for (int64_t j = h->orth_ranges[i].first; j <= h->orth_ranges[i].second; ++j) w2[j] = eps * gauss(h, 0.0, 2.0);
         }

@@ -333,6 +333,19 @@ void load_restart(nvb_handle *h, const char *dir, const char *vdir) {
     h->omega2 = o2;
     h->seeded = true;
     h->arch_n = 0;
+    h->firststep = true;
+    h->orth_ranges.clear();
+    // a file archive that already holds v_1..v_nload (the reference's nadvibs.34.0 of the run
+    // being restarted) lets re-orthogonalisation resume (Source/top.f90:572-575,582-587)
+    if (h->arch_kind == ARCH_FILE && h->harch_max >= nload) {
+        archive_ensure(h, nload);
+        if (FILE *f = std::fopen(h->arch_path.c_str(), "rb")) {
+            std::fseek(f, 0, SEEK_END);
+            const long long bytes = (long long)ftello(f);
+            std::fclose(f);
+            if (bytes >= (long long)nload * (long long)h->ntotal() * (long long)sizeof(double)) h->arch_n = nload;
+        }
+    }
     // device copies of the recurrence coefficients and the buffer scales
     grow_scalars_public(h, nload + 1);
     CK(cudaMemcpyAsync(h->d_alpha, h->alpha.data(), (nload + 1) * sizeof(double), cudaMemcpyHostToDevice, h->stream));
@@ -348,38 +361,6 @@ void load_restart(nvb_handle *h, const char *dir, const char *vdir) {
     const std::string old = rl + ".old";
     std::rename(rl.c_str(), old.c_str());
     std::remove(vf.c_str());
-}
-
-// ---------------------------------------------------------------- archive
-void archive_ensure(nvb_handle *h, int64_t need) {
-    if (h->opt.archive_max <= 0) return;
-    const int64_t cap = std::min<int64_t>(need, h->opt.archive_max);
-    if (cap <= h->arch_cap) return;
-    void *na = nullptr;
-    const size_t per = (size_t)h->ntotal() * h->elem_size();
-    CK(cudaMalloc(&na, per * cap));
-    if (h->arch && h->arch_n > 0)
-        CK(cudaMemcpyAsync(na, h->arch, per * h->arch_n, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    if (h->arch) cudaFree(h->arch);
-    h->arch = na;
-    h->arch_cap = cap;
-}
-
-// store v_it = scale[cur] * buf[cur] as archive entry it-1 (called at the start of iteration it)
-void archive_push(nvb_handle *h, int64_t it) {
-    if (!h->arch || it - 1 != h->arch_n || h->arch_n >= h->arch_cap) return;
-    const long long n = h->ntotal();
-    const size_t per = (size_t)n * h->elem_size();
-    void *dst = (char *)h->arch + per * (size_t)(it - 1);
-    if (h->precision == NVB_MIXED)
-        k_scale_copy<float><<<grid_n(n), 256, 0, h->stream>>>((const float *)h->buf[h->cur], h->d_scale + h->cur,
-                                                              (float *)dst, n);
-    else
-        k_scale_copy<double><<<grid_n(n), 256, 0, h->stream>>>((const double *)h->buf[h->cur], h->d_scale + h->cur,
-                                                               (double *)dst, n);
-    CK(cudaGetLastError());
-    h->arch_n = it;
 }
 
 // ---------------------------------------------------------------- Ritz vectors
@@ -411,17 +392,20 @@ static void ritz_vectors(nvb_handle *h, int64_t nroots, const std::vector<double
         for (int64_t j = 0; j < nroots; ++j) coef[(size_t)k * nroots + j] = V[(size_t)j * n + k];
     CK(cudaMemcpyAsync(dc, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     const bool mixed = h->precision == NVB_MIXED;
-    if (h->arch && h->arch_n >= n) {
+    if (archive_holds(h, n)) {
         const size_t per = (size_t)N * h->elem_size();
-        for (int64_t k = 0; k < n; ++k) {
-            const void *vk = (const char *)h->arch + per * k;
-            if (mixed)
-                k_ritz_accum<float><<<grid_n(N), 256, 0, h->stream>>>((const float *)vk, 1.0, dc + k * nroots,
-                                                                      (int)nroots, psi, N);
-            else
-                k_ritz_accum<double><<<grid_n(N), 256, 0, h->stream>>>((const double *)vk, 1.0, dc + k * nroots,
-                                                                       (int)nroots, psi, N);
-        }
+        archive_for_chunks(h, 1, n, [&](const void *base, int64_t first, int64_t count) {
+            for (int64_t q = 0; q < count; ++q) {
+                const int64_t k = first - 1 + q;
+                const void *vk = (const char *)base + per * q;
+                if (mixed)
+                    k_ritz_accum<float><<<grid_n(N), 256, 0, h->stream>>>((const float *)vk, 1.0, dc + k * nroots,
+                                                                          (int)nroots, psi, N);
+                else
+                    k_ritz_accum<double><<<grid_n(N), 256, 0, h->stream>>>((const double *)vk, 1.0, dc + k * nroots,
+                                                                           (int)nroots, psi, N);
+            }
+        });
     } else {
         // replay v_1..v_n from the seed with the stored alpha/beta in three scratch buffers
         const size_t per = (size_t)N * h->elem_size();

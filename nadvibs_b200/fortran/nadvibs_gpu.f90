@@ -35,6 +35,24 @@ module nadvibs_gpu
       type(c_ptr), value :: h
       integer(c_int64_t), value :: reorthog, chkorthog
     end function
+    integer(c_int) function nvb_set_archive(h, kind, max_vectors, path) bind(C, name="nvb_set_archive")
+      import :: c_int, c_int64_t, c_char, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: kind, max_vectors
+      character(kind=c_char), dimension(*), intent(in) :: path
+    end function
+    integer(c_int) function nvb_reorth_log(h, max_entries, iteration, lo, hi, count) bind(C, name="nvb_reorth_log")
+      import :: c_int, c_int64_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: max_entries
+      integer(c_int64_t), intent(out) :: iteration(*), lo(*), hi(*), count
+    end function
+    integer(c_int) function nvb_reorth_omega(h, n, omega1, omega2, omega2_step) bind(C, name="nvb_reorth_omega")
+      import :: c_int, c_int64_t, c_double, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: n
+      real(c_double), intent(out) :: omega1(*), omega2(*), omega2_step(*)
+    end function
     integer(c_int) function nvb_write_header(h, path) bind(C, name="nvb_write_header")
       import :: c_int, c_char, c_ptr
       type(c_ptr), value :: h

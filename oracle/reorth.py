@@ -13,7 +13,36 @@ from __future__ import annotations
 import numpy as np
 
 
-def lanczos_reorth_exact(S, niter: int, weights=None):
+def choose_intervals(om2, it: int, eps: float = 2.0 ** -53):
+    """partial_orthog's intervals (Source/top.f90:915-968) from omega(2, 0:it): around every i with
+    |omega| >= sqrt(eps), widened while |omega| >= eps^(3/4), duplicates of the previous interval's
+    ends dropped, and (1, 1) added when no interval starts at 1."""
+    eta = eps ** 0.75
+    oi = [i for i in range(1, it + 1) if abs(om2[i]) >= np.sqrt(eps)]
+    ranges = []
+    if oi:
+        lid, rid = [], []
+        for o in oi:
+            j = o
+            while j >= 1 and not abs(om2[j]) < eta:
+                j -= 1
+            lid.append(max(j, 1))
+            k = o
+            while k <= it and not abs(om2[k]) < eta:
+                k += 1
+            rid.append(min(k, it))
+        ranges = [(lid[0], rid[0])]
+        for a, b in zip(lid[1:], rid[1:]):
+            if a != ranges[-1][0] and b != ranges[-1][1]:
+                ranges.append((a, b))
+        if min(r[0] for r in ranges) > 1:
+            ranges.append((1, 1))
+    return ranges
+
+
+def lanczos_reorth_exact(S, niter: int, weights=None, log=None):
+    """alpha[1..n], beta[0..n] and the Lanczos vectors; with a list `log`, every interval
+    partial_orthog orthogonalises against is appended as (iteration, lo, hi), 1-based."""
     eps = 2.0 ** -53
     eta = eps ** 0.75
     N = S.ntotal
@@ -50,26 +79,10 @@ def lanczos_reorth_exact(S, niter: int, weights=None):
         for i in range(1, it + 1):
             om2[i] = q3 @ V[i - 1]
         if firststep:
-            oi = [i for i in range(1, it + 1) if abs(om2[i]) >= np.sqrt(eps)]
-            ranges = []
-            if oi:
-                lid, rid = [], []
-                for o in oi:
-                    j = o
-                    while j >= 1 and not abs(om2[j]) < eta:
-                        j -= 1
-                    lid.append(max(j, 1))
-                    k = o
-                    while k <= it and not abs(om2[k]) < eta:
-                        k += 1
-                    rid.append(min(k, it))
-                ranges = [(lid[0], rid[0])]
-                for a, b in zip(lid[1:], rid[1:]):
-                    if a != ranges[-1][0] and b != ranges[-1][1]:
-                        ranges.append((a, b))
-                if min(r[0] for r in ranges) > 1:
-                    ranges.append((1, 1))
+            ranges = choose_intervals(om2, it, eps)
         if ranges:
+            if log is not None:
+                log.extend((it, a, b) for a, b in ranges)
             dots = [[q3 @ V[j - 1] for j in range(a, b + 1)] for a, b in ranges]
             for (a, b), d in zip(ranges, dots):
                 for j, c in zip(range(a, b + 1), d):
