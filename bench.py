@@ -42,10 +42,19 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both")
     ap.add_argument("--hv-only", action="store_true", help="run H.v launches only (profiling)")
+    ap.add_argument("--grad-only", action="store_true",
+                    help="run the gradient leg only and print its JSON (profiling)")
     ap.add_argument("--config", type=int, default=CONFIG_NUMBER)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient (grad/fwd) measurement")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the mixed-vs-FP64 Ritz comparison")
+    ap.add_argument("--no-fma", action="store_true", help="skip the measured FMA ceilings")
+    ap.add_argument("--no-config5", action="store_true",
+                    help="skip the short literal-size run of the cubic system (config 5)")
+    ap.add_argument("--no-reorth", action="store_true",
+                    help="skip the re-orthogonalised mixed run with the host-memory archive")
+    ap.add_argument("--reorth-iters", type=int, default=150,
+                    help="iterations of the re-orthogonalised run (capped by host memory)")
     ap.add_argument("--config5", action="store_true",
                     help="also run the large cubic system (config 5): literal-size mixed forward and the "
                          "budgeted gradient (minutes; not part of the default run)")
@@ -264,6 +273,56 @@ def mixed_accuracy(basis: str, nadvibs: str, dev: int, iters: int = 2000, nroots
             "wall_s": {"fp64": secs[L.NVB_FP64], "mixed": secs[L.NVB_MIXED]}}
 
 
+def host_available_bytes() -> int:
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def reorth_leg(basis: str, nadvibs: str, dev: int, iters: int = 150, host_frac: float = 0.6):
+    """The re-orthogonalised mixed-precision run (the config-2 Hamiltonian with FP32 vectors,
+    reorthog=1: the omega recurrence with exact checks every chkorthog=100 iterations, partial
+    re-orthogonalisation), its Lanczos-vector archive in pinned host memory streamed back to the
+    GPU in chunks.  One vector is 1.06 GB, so the run is as long as `host_frac` of the host's
+    available memory allows (at most `iters`); the reference keeps the same archive on disk.
+    Reports iter/s (including pinning the archive), the re-orthogonalisation events, and the
+    converged roots with the smallest gap between two of them (no ghost copies)."""
+    import numpy as np
+    from nadvibs_b200 import _lib as L
+    au2cm = 219474.6313705
+    h = L.Handle.from_files(basis, nadvibs, device=dev, precision=L.NVB_MIXED)
+    try:
+        sz = h.sizes()
+        per = int(sz["dimen"]) * int(sz["nstates"]) * 4
+        fit = int(host_frac * host_available_bytes() // per)
+        n = max(0, min(iters, fit))
+        if n < 10:
+            return {"skipped": f"host memory for {n} archived vectors only"}
+        h.set_archive(1, n)
+        h.set_reorthog(1, 100)
+        t0 = time.perf_counter()
+        h.seed()
+        h.lanczos(n)
+        dt = time.perf_counter() - t0
+        log = h.reorth_log()
+        E, bji, inten = h.ritz(n)[:3]
+    finally:
+        h.close()
+    conv = np.sort(E[bji < 1e-8])
+    return {"iterations": n, "archive": "pinned host memory", "archive_gb": n * per / 1e9,
+            "host_available_gb": host_available_bytes() / 1e9, "host_fraction_used": host_frac,
+            "wall_s": dt, "iter_per_s": n / dt,
+            "reorth_events": int(len(set(int(r[0]) for r in log))),
+            "vectors_reorthogonalised": int(sum(int(r[2]) - int(r[1]) + 1 for r in log)),
+            "converged_roots": int(conv.size),
+            "min_gap_converged_cm": float(np.diff(conv).min() * au2cm) if conv.size > 1 else None}
+
+
 def grad_timing(dev: int):
     """grad/fwd on the gradient system (config 4): forward = seed + 400 plain Lanczos
     iterations, recording every Lanczos vector and H v for the reverse sweep (checkpoint
@@ -329,7 +388,8 @@ def grad_timing(dev: int):
             "grad_over_fwd": g / f}
 
 
-def large_cubic(dev: int, iters: int = 4, warm: int = 2, grad_iters: int = 60, budget: float = 150e9):
+def large_cubic(dev: int, iters: int = 4, warm: int = 2, grad_iters: int = 60, budget: float = 150e9,
+                with_grad: bool = True):
     """Config 5, ordr 3 (cubic terms N(0,10 cm^-1)), 3 states, 10 modes, FP32 vectors / FP64
     recurrence.  (1) The literal basis [16,14,12,10,8,8,6,6,4,4]: 990,904,320 functions per
     state, 2,972,712,960 elements, 11.9 GB per FP32 vector; `warm` + `iters` mixed iterations,
@@ -370,6 +430,8 @@ def large_cubic(dev: int, iters: int = 4, warm: int = 2, grad_iters: int = 60, b
                           "device_gb_in_use_after_create": (total - free) / 1e9, "iterations_timed": iters}
     finally:
         h.close()
+    if not with_grad:
+        return out
     basis = [8, 7, 6, 10, 8, 8, 6, 6, 4, 4]
     n = grad_iters
     h = L.Handle.from_arrays(params(basis, n), om, cc, potf, device=dev, precision=L.NVB_MIXED)
@@ -484,6 +546,12 @@ def main():
                                             "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
+    if args.grad_only:
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps({"grad": grad_timing(local)}))
+        return 0
     if world > 1:
         from nadvibs_b200 import replicas
         replicas.init("nccl", timeout_s=120)
@@ -526,14 +594,41 @@ def main():
                        "achieved_tflops": fl / (r["hv_ms_per"] / 1e3) / 1e12, "precision": main_prec}
         if "mixed" in res and main_prec != "mixed":
             line["alu"]["mixed_achieved_tflops"] = fl / (res["mixed"]["hv_ms_per"] / 1e3) / 1e12
+        if not args.no_fma:
+            # measured FMA ceilings of this GPU (seconds-long register-only FMA loops), against
+            # which the reference-equivalent flop rates above are compared
+            import torch
+            from nadvibs_b200 import _lib as L
+            torch.cuda.set_device(local)
+            f64 = L.measure_fma(L.DTYPE_F64, 2.0)
+            f32 = L.measure_fma(L.DTYPE_F32, 2.0)
+            line["alu"]["measured_fp64_tflops"] = f64 / 1e12
+            line["alu"]["measured_fp32_tflops"] = f32 / 1e12
+            line["alu"]["frac_of_measured_fp64"] = line["alu"]["achieved_tflops"] / (f64 / 1e12)
+            if "mixed_achieved_tflops" in line["alu"]:
+                line["alu"]["mixed_frac_of_measured_fp32"] = line["alu"]["mixed_achieved_tflops"] / (f32 / 1e12)
     if rank == 0 and not args.no_grad:
         line["grad"] = grad_timing(local)
     if rank == 0 and args.config5:
         line["config5"] = large_cubic(local)
+    elif rank == 0 and not args.no_config5:
+        # the cubic system at its literal size: a few mixed iterations (the gradient at the
+        # stated size runs with --config5)
+        try:
+            line["config5"] = large_cubic(local, iters=2, warm=1, with_grad=False)
+        except Exception as e:
+            line["config5"] = {"error": str(e)}
     if rank == 0 and "mixed" in res and not args.no_accuracy:
         tmp = tempfile.mkdtemp(prefix="nvb_acc_")
         _, (b_in, n_in) = make_inputs(args.config, tmp, args.basis)
         line["accuracy"] = mixed_accuracy(b_in, n_in, local)
+    if rank == 0 and "mixed" in res and not args.no_reorth:
+        tmp = tempfile.mkdtemp(prefix="nvb_reorth_")
+        _, (b_in, n_in) = make_inputs(args.config, tmp, args.basis)
+        try:
+            line["reorth"] = reorth_leg(b_in, n_in, local, args.reorth_iters)
+        except Exception as e:  # reported, not fatal: the leg needs ~100 GB of pinned host memory
+            line["reorth"] = {"error": str(e)}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(args.config, 1)
     if rank == 0:

@@ -340,6 +340,12 @@ int nvb_dot(nvb_handle *h, const void *a, double sa, const void *b, double sb, i
 int nvb_dot_noalloc(const void *a, double sa, const void *b, double sb, int64_t n, int64_t dtype, double *result_dev,
                     void *stream);
 
+/* Measured FMA throughput of the current device's CUDA cores (no reference counterpart): a
+ * register-only kernel of independent FMA chains, repeated for about `seconds` of device time
+ * and timed with CUDA events; *flops_per_s = 2 x FMAs / s for dtype NVB_DTYPE_F64 or
+ * NVB_DTYPE_F32.  The arithmetic ceiling the H.v kernels' flops are compared with. */
+int nvb_measure_fma(int64_t dtype, double seconds, double *flops_per_s);
+
 /* Per-phase device timing of nvb_lanczos (the reference writes per-phase wall times to
  * output.dat, Source/top.f90:663-667,814-817,834-841): when enabled, CUDA events on the
  * handle's stream bracket the H.v launch and the whole iteration; nvb_get_timing returns

@@ -56,6 +56,7 @@ _SIGS = {
     "nvb_set_archive": [C.c_void_p, C.c_int64, C.c_int64, C.c_char_p],
     "nvb_reorth_log": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_reorth_omega": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p],
+    "nvb_measure_fma": [C.c_int64, C.c_double, C.c_void_p],
     "nvb_set_fault_test": [C.c_void_p, C.c_int64],
     "nvb_set_displaced_seed": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_seed_overlap": [C.c_void_p, C.c_void_p],
@@ -121,6 +122,13 @@ def dot_noalloc(a_ptr: int, b_ptr: int, n: int, dtype: int, result_ptr: int, str
     """nvb_dot_noalloc: <sa*a, sb*b> written to the device double at result_ptr (no allocation)."""
     check(lib().nvb_dot_noalloc(C.c_void_p(a_ptr), sa, C.c_void_p(b_ptr), sb, n, dtype, C.c_void_p(result_ptr),
                                 C.c_void_p(stream_ptr) if stream_ptr else None))
+
+
+def measure_fma(dtype: int, seconds: float = 2.0) -> float:
+    """nvb_measure_fma: FMA throughput of the current device (flop/s, 2 per FMA)."""
+    r = C.c_double()
+    check(lib().nvb_measure_fma(dtype, seconds, C.byref(r)))
+    return r.value
 
 
 SHAPE_FWHM_GAUSSIAN, SHAPE_GAUSSIAN, SHAPE_LORENTZIAN = 0, 1, 2

@@ -53,6 +53,12 @@ module nadvibs_gpu
       integer(c_int64_t), value :: n
       real(c_double), intent(out) :: omega1(*), omega2(*), omega2_step(*)
     end function
+    integer(c_int) function nvb_measure_fma(dtype, seconds, flops_per_s) bind(C, name="nvb_measure_fma")
+      import :: c_int, c_int64_t, c_double
+      integer(c_int64_t), value :: dtype
+      real(c_double), value :: seconds
+      real(c_double), intent(out) :: flops_per_s
+    end function
     integer(c_int) function nvb_write_header(h, path) bind(C, name="nvb_write_header")
       import :: c_int, c_char, c_ptr
       type(c_ptr), value :: h
