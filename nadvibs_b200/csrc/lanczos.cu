@@ -69,16 +69,41 @@ __global__ void k_finalize(const double *__restrict__ part, int n, double *out, 
     }
 }
 
-template <typename T>
-__global__ void k_passB(T *__restrict__ w, const T *__restrict__ c, const T *__restrict__ p,
-                        const double *__restrict__ sc, const double *__restrict__ sp,
-                        const double *__restrict__ alpha, const double *__restrict__ beta_prev, long long n,
-                        double *__restrict__ part) {
+// Pass B, r = w - alpha v_i - beta_{i-1} v_{i-1} in place of w with partial sums of ||r||^2
+// (FP64 arithmetic, r rounded to the buffers' type and the norm taken from the rounded values),
+// with W-element vector accesses (float4 / double2: 16 bytes per load and store, so that enough
+// bytes are in flight to stream at the HBM copy rate); elements beyond the last whole vector
+// are done one by one.
+template <typename T, typename V, int W>
+__global__ void k_passB_vec(T *__restrict__ w, const T *__restrict__ c, const T *__restrict__ p,
+                            const double *__restrict__ sc, const double *__restrict__ sp,
+                            const double *__restrict__ alpha, const double *__restrict__ beta_prev, long long n,
+                            double *__restrict__ part) {
     const double a = *alpha * *sc;
     const double b = *beta_prev * *sp;
     double acc = 0.0;
+    const long long nvec = n / W;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    V *wv = reinterpret_cast<V *>(w);
+    const V *cv = reinterpret_cast<const V *>(c);
+    const V *pv = reinterpret_cast<const V *>(p);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nvec; i += stride) {
+        V x = wv[i];
+        const V y = cv[i], z = pv[i];
+        T *xs = reinterpret_cast<T *>(&x);
+        const T *ys = reinterpret_cast<const T *>(&y);
+        const T *zs = reinterpret_cast<const T *>(&z);
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+            double r = (double)xs[q] - a * (double)ys[q];
+            r = r - b * (double)zs[q];
+            const T rt = (T)r;
+            xs[q] = rt;
+            acc += (double)rt * (double)rt;
+        }
+        wv[i] = x;
+    }
+    for (long long i = nvec * W + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         double r = (double)w[i] - a * (double)c[i];
         r = r - b * (double)p[i];
         const T rt = (T)r;
@@ -350,10 +375,15 @@ template <typename T>
 static void passB_launch(nvb_handle *h, int64_t it, int *blocks) {
     const long long n = h->ntotal();
     const int g = grid_for(n);
-    k_passB<T><<<g, RED_THREADS, 0, h->stream>>>((T *)h->buf[h->work], (const T *)h->buf[h->cur],
-                                                 (const T *)h->buf[h->prev], h->d_scale + h->cur,
-                                                 h->d_scale + h->prev, h->d_alpha + it, h->d_beta + it - 1, n,
-                                                 h->d_part);
+    // the three buffers are cudaMalloc'd (256-byte aligned): 16-byte vector accesses
+    if constexpr (sizeof(T) == 4)
+        k_passB_vec<float, float4, 4><<<g, RED_THREADS, 0, h->stream>>>(
+            (float *)h->buf[h->work], (const float *)h->buf[h->cur], (const float *)h->buf[h->prev],
+            h->d_scale + h->cur, h->d_scale + h->prev, h->d_alpha + it, h->d_beta + it - 1, n, h->d_part);
+    else
+        k_passB_vec<double, double2, 2><<<g, RED_THREADS, 0, h->stream>>>(
+            (double *)h->buf[h->work], (const double *)h->buf[h->cur], (const double *)h->buf[h->prev],
+            h->d_scale + h->cur, h->d_scale + h->prev, h->d_alpha + it, h->d_beta + it - 1, n, h->d_part);
     *blocks = g;
 }
 
