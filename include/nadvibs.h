@@ -194,6 +194,13 @@ int nvb_ritz(nvb_handle *h, int64_t n, double *E, double *bji, double *inten, in
  * for T_n, n = iters, with bjiconv = 10^-bconv from basis.in, appending to path. */
 int nvb_write_eigenvalues(nvb_handle *h, const char *path);
 
+/* Append the seed section of output.dat after nvb_seed (generate_initialvec's report,
+ * Source/secondary.f90:351-802): for a displaced seed (shiftref != 0) the number of basis
+ * functions per quanta-sum level and the <m| levels built; for either seed the overlap with the
+ * initial state, its (up to) 40 dominant basis functions with their quanta, the normalisation
+ * of the initial Lanczos vector by the state weights and the time nvb_seed took. */
+int nvb_write_seed_report(nvb_handle *h, const char *path);
+
 /* Write the output.dat header for the job (print_basis, Source/top.f90:248-342), replacing
  * path. */
 int nvb_write_header(nvb_handle *h, const char *path);

@@ -57,6 +57,7 @@ _SIGS = {
     "nvb_reorth_log": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_reorth_omega": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_measure_fma": [C.c_int64, C.c_double, C.c_void_p],
+    "nvb_write_seed_report": [C.c_void_p, C.c_char_p],
     "nvb_set_fault_test": [C.c_void_p, C.c_int64],
     "nvb_set_displaced_seed": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_seed_overlap": [C.c_void_p, C.c_void_p],
@@ -314,6 +315,10 @@ class Handle:
         n = nroots * k
         return dict(state=st[:n].reshape(nroots, k), index=ix[:n].reshape(nroots, k),
                     c2=c2[:n].reshape(nroots, k), phase=ph[:n].reshape(nroots, k), pct=pct.reshape(nroots, S))
+
+    def write_seed_report(self, path: str):
+        """Append the seed section of output.dat (nvb_write_seed_report)."""
+        check(lib().nvb_write_seed_report(self.ptr, path.encode()))
 
     def set_reorthog(self, reorthog: int, chkorthog: int = 100):
         check(lib().nvb_set_reorthog(self.ptr, reorthog, chkorthog))

@@ -304,7 +304,17 @@ int nvb_seed(nvb_handle *h, const double *weights) {
     return guarded([&] {
         if (!h) fail(NVB_ERR_ARG, "null handle");
         ensure_device(h);
+        const auto t0 = std::chrono::steady_clock::now();
         lanczos_seed(h, weights);
+        h->seed_secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    });
+}
+
+int nvb_write_seed_report(nvb_handle *h, const char *path) {
+    return guarded([&] {
+        if (!h || !path) fail(NVB_ERR_ARG, "null argument");
+        ensure_device(h);
+        write_seed_report(h, path);
     });
 }
 

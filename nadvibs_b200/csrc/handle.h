@@ -83,6 +83,7 @@ struct nvb_handle {
     // displaced / Duschinsky seed: <m|n> over one state block (FP64) and its norm
     double *seed_vec = nullptr;
     double seed_norm = 0.0;
+    double seed_secs = 0.0;  // wall time of the last nvb_seed (the seed report's "Time Required")
     // cached scratch for ad-hoc vectors
     void *tmp = nullptr;
     size_t tmp_bytes = 0;
@@ -144,4 +145,5 @@ void lead_contributors(nvb_handle *h, int64_t nroots, int64_t k, int64_t *state,
                        int64_t *phase, double *pct, const char *rootinfo);
 void spin_orbit(nvb_handle *h, int64_t soroots, int64_t nroots, double *e_ev, double *amp, double *ov,
                 const char *path);
+void write_seed_report(nvb_handle *h, const char *path);
 }  // namespace nvb

@@ -665,3 +665,122 @@ void spin_orbit(nvb_handle *h, int64_t soroots, int64_t nroots, double *e_ev, do
 }
 
 }  // namespace nvb
+
+namespace nvb {
+
+// The seed section of output.dat (generate_initialvec's report, Source/secondary.f90:351-802,
+// formats 1000-1011 and 1022-1025): for the displaced seed the number of basis functions of
+// every quanta sum ("level") and the <m| levels built, for either seed the overlap with the
+// initial state, its 40 dominant basis functions (repeated argmax of q^2 with the row zeroed in
+// every state), and the normalisation of the initial Lanczos vector by the state weights.
+void write_seed_report(nvb_handle *h, const char *path) {
+    if (!h->seeded) fail(NVB_ERR_STATE, "nvb_write_seed_report needs nvb_seed first");
+    const System &sys = h->sys;
+    const int S = sys.S, M = sys.M;
+    const long long N = sys.dimen;
+    FILE *f = std::fopen(path, "a");
+    if (!f) fail(NVB_ERR_IO, std::string("cannot open ") + path);
+    const std::string stars(70, '*');
+    double d1 = 1.0;  // sqrt(<q3,q3>/nstates) of the unscaled seed
+    if (sys.neworigin) {
+        std::fprintf(f, "\n  %s\n  Generating seed vector by computing ANION/ORIGIN overlap...\n", stars.c_str());
+        // basis functions per quanta sum (level-synchronous recursion over sum_k n_k)
+        std::vector<long long> cnt(1, 1);
+        for (int k = 0; k < M; ++k) {
+            const int nf = (int)sys.nfunc[k];
+            std::vector<long long> nx(cnt.size() + nf - 1, 0);
+            for (size_t l = 0; l < cnt.size(); ++l)
+                for (int q = 0; q < nf; ++q) nx[l + q] += cnt[l];
+            cnt.swap(nx);
+        }
+        const int nlev = (int)cnt.size() - 1;
+        long long tcount = 0;
+        for (int j = 0; j < nlev; ++j) {
+            std::fprintf(f, "  LEVEL %s, Number of terms:     %s\n", fI(j, 5).c_str(), fI(cnt[(size_t)j], 12).c_str());
+            tcount += cnt[(size_t)j];
+        }
+        std::fprintf(f, "  LEVEL %s, Number of terms:     %s\n", fI(nlev, 5).c_str(), fI(1, 12).c_str());
+        tcount += 1;
+        std::fprintf(f, "\n  Sum over levels:                  %s\n  Size of direct product basis:     %s\n\n",
+                     fI(tcount, 12).c_str(), fI(N, 12).c_str());
+        int imode = M - 1;
+        for (int i = 0; i < M; ++i)
+            if (sys.istate[(size_t)i] > 0) {
+                imode = i;
+                break;
+            }
+        for (int64_t i = 1; i <= sys.istate[(size_t)imode]; ++i)
+            std::fprintf(f, "  Building <m| = <%s|\n", fI(i, 2).c_str());
+        d1 = h->seed_norm;
+    } else {
+        std::fprintf(f, "\n  %s\n  Generating seed vector using ANION basis...\n", stars.c_str());
+    }
+    std::fprintf(f, "\n  Overlap with the initial state:   %s\n", fF(d1, 12, 6).c_str());
+    std::fprintf(f, "\n  Dominant Contributions to Overlap\n  ---------------------------------\n");
+    // every state holds the same unscaled seed: the simple one is 1 at the first row, the
+    // displaced one <m|n>
+    auto quanta = [&](long long row) {
+        std::string s;
+        long long rem = row;
+        for (int k = 0; k < M; ++k) {
+            const long long d = rem / sys.shft[(size_t)k];
+            rem -= d * sys.shft[(size_t)k];
+            s += fI(d, 2) + ",";
+        }
+        return s;
+    };
+    if (sys.neworigin && h->seed_vec) {
+        const int nb = (int)std::min<long long>((N + 255) / 256, 1024);
+        unsigned char *taken = nullptr;
+        double *bval = nullptr;
+        long long *bidx = nullptr;
+        CK(cudaMalloc((void **)&taken, (size_t)N));
+        CK(cudaMalloc((void **)&bval, nb * sizeof(double)));
+        CK(cudaMalloc((void **)&bidx, nb * sizeof(long long)));
+        CK(cudaMemsetAsync(taken, 0, (size_t)N, h->stream));
+        std::vector<double> hv(nb);
+        std::vector<long long> hi(nb);
+        for (int sidx = 1; sidx <= 40; ++sidx) {
+            k_argmax_sq<<<nb, 256, 0, h->stream>>>(h->seed_vec, taken, N, bval, bidx);
+            CK(cudaMemcpyAsync(hv.data(), bval, nb * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(hi.data(), bidx, nb * sizeof(long long), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            double best = -1.0;
+            long long bi = -1;
+            for (int q = 0; q < nb; ++q)
+                if (hi[q] >= 0 && (hv[q] > best || (hv[q] == best && hi[q] < bi))) {
+                    best = hv[q];
+                    bi = hi[q];
+                }
+            if (bi < 0 || best == 0.0) break;
+            const unsigned char one = 1;
+            CK(cudaMemcpy(taken + bi, &one, 1, cudaMemcpyHostToDevice));
+            std::fprintf(f, "  %s. %s: %s\n", fI(sidx, 2).c_str(), quanta(bi).c_str(), fF(best, 12, 6).c_str());
+        }
+        cudaFree(taken);
+        cudaFree(bval);
+        cudaFree(bidx);
+    } else {
+        std::fprintf(f, "  %s. %s: %s\n", fI(1, 2).c_str(), quanta(0).c_str(), fF(1.0, 12, 6).c_str());
+    }
+    // the state weights scale the blocks, then the vector is normalised
+    double wsum = 0.0;
+    for (double w : h->seed_w) wsum += w;
+    if (wsum == 0.0) wsum = 1.0;
+    std::fprintf(f, "\n  Normalization of Initial Lanczos Vector\n");
+    double tot = 0.0;
+    for (int s = 0; s < S; ++s) {
+        const double n = std::fabs(h->seed_w[(size_t)s] / wsum);
+        tot += n * n;
+        std::fprintf(f, "  ||STATE%s|| = %s -- (||STATE%s||)^2 = %s\n", fI(s + 1, 2).c_str(), fF(n, 6, 4).c_str(),
+                     fI(s + 1, 2).c_str(), fF(n * n, 6, 4).c_str());
+    }
+    std::fprintf(f, "  || TOTAL || = %s -- (|| TOTAL ||)^2 = %s\n", fF(std::sqrt(tot), 6, 4).c_str(),
+                 fF(tot, 6, 4).c_str());
+    std::fprintf(f, "  Normalizing Initial Lanczos Vector...\n");
+    std::fprintf(f, "  || TOTAL || = %s -- (|| TOTAL ||)^2 = %s\n", fF(1.0, 6, 4).c_str(), fF(1.0, 6, 4).c_str());
+    std::fprintf(f, "\n  Time Required: %s secs.\n  %s\n\n", fF(h->seed_secs, 14, 3).c_str(), stars.c_str());
+    std::fclose(f);
+}
+
+}  // namespace nvb

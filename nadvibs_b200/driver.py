@@ -66,6 +66,7 @@ def run(workdir: str = ".", outdir: str | None = None, precision: str = "fp64", 
             log(f"Restarting Lanczos procedure on step {iters_before + 1}")
         else:
             h.seed()
+            h.write_seed_report(out)
         h.set_timing(True)
         a, b = h.lanczos(params.niter)
         hv_ms, it_ms, n = h.timing()

@@ -59,6 +59,11 @@ module nadvibs_gpu
       real(c_double), value :: seconds
       real(c_double), intent(out) :: flops_per_s
     end function
+    integer(c_int) function nvb_write_seed_report(h, path) bind(C, name="nvb_write_seed_report")
+      import :: c_int, c_char, c_ptr
+      type(c_ptr), value :: h
+      character(kind=c_char), dimension(*), intent(in) :: path
+    end function
     integer(c_int) function nvb_write_header(h, path) bind(C, name="nvb_write_header")
       import :: c_int, c_char, c_ptr
       type(c_ptr), value :: h

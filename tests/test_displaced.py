@@ -110,3 +110,71 @@ def test_gpu_displaced_seed_from_files_and_replay(tmp_path):
         h.lanczos(15)
         archived = h.lead_contributors(3, 4)
     np.testing.assert_allclose(two_pass["c2"], archived["c2"], rtol=1e-10, atol=1e-14)
+
+
+def _report_lines(path):
+    with open(path) as f:
+        return f.read().splitlines()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("istate", [[0, 0, 0], [0, 2, 0]])
+def test_gpu_seed_report_of_the_displaced_seed(istate, tmp_path):
+    """The seed section of output.dat (Source/secondary.f90:351-802) for a displaced seed: one
+    line per quanta-sum level whose counts add up to the basis size, the <m| levels built, the
+    overlap with the initial state, the dominant basis functions in the reference's format
+    ('  NN. q,q,q,: value') equal to the oracle's 40 largest <m|n>^2, and the normalisation by
+    the state weights."""
+    L, p, om, cc, potf, disp, S, ov, cfg = _gpu_case(82, 2, [5, 4, 3], istate)
+    out = str(tmp_path / "output.dat")
+    w = np.array([1.0, 0.5])
+    with L.Handle.from_arrays(p, om, cc, potf, quirk_lower=0) as h:
+        h.set_displaced_seed(*disp)
+        h.seed(w)
+        h.write_seed_report(out)
+    lines = _report_lines(out)
+    assert "  Generating seed vector by computing ANION/ORIGIN overlap..." in lines
+    levels = [ln for ln in lines if ln.startswith("  LEVEL ")]
+    assert len(levels) == (5 - 1) + (4 - 1) + (3 - 1) + 1
+    assert sum(int(ln.split()[-1]) for ln in levels) == 5 * 4 * 3
+    assert [ln for ln in lines if ln.startswith("  Building <m|")] == \
+        [f"  Building <m| = <{i:2d}|" for i in range(1, max(istate) + 1)]
+    ovl = [ln for ln in lines if ln.startswith("  Overlap with the initial state:")]
+    assert float(ovl[0].split(":")[1]) == pytest.approx(np.linalg.norm(ov), abs=1e-6)
+    dom = [ln for ln in lines if len(ln) > 5 and ln[4] == "." and ln[:4].strip().isdigit()]
+    order = np.argsort(-ov ** 2, kind="stable")[:40]
+    assert len(dom) == min(40, int((ov != 0).sum()))
+    for k, (ln, row) in enumerate(zip(dom, order)):
+        head, val = ln.rsplit(":", 1)
+        assert head.startswith(f"  {k + 1:2d}. ")
+        quanta = [int(t) for t in head[6:].split(",") if t.strip()]
+        assert quanta == [row // 12, (row // 3) % 4, row % 3]
+        assert float(val) == pytest.approx(ov[row] ** 2, abs=1e-6)
+    norms = [ln for ln in lines if ln.startswith("  ||STATE")]
+    q = w / w.sum()
+    for s, ln in enumerate(norms):
+        assert float(ln.split("=")[1].split("--")[0]) == pytest.approx(q[s], abs=1e-4)
+    assert lines.count("  Normalizing Initial Lanczos Vector...") == 1
+
+
+@pytest.mark.gpu
+def test_gpu_seed_report_of_the_origin_seed(tmp_path):
+    """shiftref = 0: the report of the reference's simple seed (the ground state of every
+    electronic state): overlap 1, one dominant contribution (all quanta 0, weight 1)."""
+    from nadvibs_b200 import _lib as L
+    from nadvibs_b200 import synth
+    cfg = synth.config(1)
+    om, cc, pot = synth.draw(cfg)
+    p = L.default_params()
+    p.nstates, p.nmodes, p.ordr = cfg.nstates, cfg.nmodes, cfg.ordr
+    for i, b in enumerate(cfg.basis):
+        p.basis[i] = b
+    out = str(tmp_path / "output.dat")
+    with L.Handle.from_arrays(p, om, cc, synth.flatten_pot(pot)) as h:
+        h.seed()
+        h.write_seed_report(out)
+    lines = _report_lines(out)
+    assert "  Generating seed vector using ANION basis..." in lines
+    assert "  Overlap with the initial state:       1.000000" in lines
+    assert "   1.  0, 0, 0, 0,:     1.000000" in lines
+    assert "  || TOTAL || = 1.0000 -- (|| TOTAL ||)^2 = 1.0000" in lines
