@@ -69,9 +69,11 @@ typedef struct nvb_options {
     int64_t archive_max;   /* max Lanczos vectors kept on the device for Ritz vectors /
                               re-orthogonalisation; 0 = none (two-pass Ritz vectors) */
     int64_t hv_kernel;     /* 0 = automatic choice (factorised quadratic kernel where the
-                              system suits it, else the slab-tiled kernel, else gather);
-                              1 = gather kernel; 2 = slab-tiled kernel; 3 = factorised
-                              quadratic kernel (ordr <= 2, state-diagonal bilinear terms) */
+                              system suits it, else the factorised cubic kernel, else the
+                              slab-tiled kernel, else gather); 1 = gather kernel; 2 = slab-tiled
+                              kernel; 3 = factorised quadratic kernel (ordr <= 2, state-diagonal
+                              bilinear terms); 4 = factorised cubic kernel (ordr <= 3, couplings
+                              between different states constant or linear) */
     int64_t seed;          /* seed of the omega-recurrence noise (the reference is unseeded) */
 } nvb_options;
 
@@ -106,7 +108,8 @@ int nvb_get_sizes(nvb_handle *h, int64_t *dimen, int64_t *nstates, int64_t *nmod
                   int64_t *npot, int64_t *iters);
 
 /* Which H.v kernel a product with vectors of this dtype runs (16-byte aligned vectors):
- * 1 = gather, 2 = slab-tiled, 3 = factorised quadratic.  No reference counterpart (the
+ * 1 = gather, 2 = slab-tiled, 3 = factorised quadratic, 4 = factorised cubic.  No reference
+ * counterpart (the
  * reference has one product routine, Source/top.f90:672-818). */
 int nvb_hv_kernel_in_use(nvb_handle *h, int64_t dtype, int64_t *kernel);
 
@@ -129,7 +132,7 @@ int nvb_set_stream(nvb_handle *h, void *stream);
 int nvb_synchronize(nvb_handle *h);
 
 /* Failure-detection test hook (no reference counterpart): mode 1 makes the factorised
- * quadratic H.v kernel issue none of its copies, so every wait of its consumer warps runs out
+ * quadratic and cubic H.v kernels issue none of their copies, so every wait of its consumer warps runs out
  * (after a short poll limit in this mode); the kernel raises its abort flag, finishes without
  * touching the missing data and sets its error word, which the next nvb_synchronize /
  * nvb_lanczos reports as NVB_ERR_CUDA.  Mode 0 (default) restores normal operation. */

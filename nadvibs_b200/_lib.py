@@ -213,10 +213,10 @@ class Handle:
         return dict(zip(("dimen", "nstates", "nmodes", "nterms", "npot", "iters"), [x.value for x in v]))
 
     def hv_kernel(self, dtype: int = DTYPE_F64) -> str:
-        """Name of the H.v kernel products of this dtype run: gather, slab or quad."""
+        """Name of the H.v kernel products of this dtype run: gather, slab, quad or cubic."""
         k = C.c_int64()
         check(lib().nvb_hv_kernel_in_use(self.ptr, dtype, C.byref(k)))
-        return {1: "gather", 2: "slab", 3: "quad"}[k.value]
+        return {1: "gather", 2: "slab", 3: "quad", 4: "cubic"}[k.value]
 
     def terms(self):
         sz = self.sizes()

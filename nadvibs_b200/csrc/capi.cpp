@@ -120,6 +120,11 @@ static void create_common(nvb_handle *h, const nvb_params &p, const double *omeg
         if (h->opt.hv_kernel == 3 && !h->quad.ok)
             fail(NVB_ERR_ARG, "factorised quadratic kernel requested but the system does not suit it");
     }
+    if ((h->opt.hv_kernel == 0 && !h->quad.ok) || h->opt.hv_kernel == 4) {
+        if (nvb::cubic_build(h->cubic, h->plan, h->sys, (int)h->opt.quirk_cubic)) nvb::cubic_upload(h->cubic);
+        if (h->opt.hv_kernel == 4 && !h->cubic.ok)
+            fail(NVB_ERR_ARG, "factorised cubic kernel requested but the system does not suit it");
+    }
     if (h->opt.hv_kernel == 0 || h->opt.hv_kernel == 2) {
         for (int i = 0; i < 2; ++i)
             if (slab_build(h->slab[i], h->plan, h->sys, (int)h->opt.quirk_cubic, i == 0 ? 8 : 4)) slab_upload(h->slab[i]);
@@ -185,6 +190,7 @@ int nvb_destroy(nvb_handle *h) {
             slab_free(h->slab[0]);
             slab_free(h->slab[1]);
             quad_free(h->quad);
+            cubic_free(h->cubic);
             ckpt_free(h);
             if (h->seed_vec) cudaFree(h->seed_vec);
             if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -202,6 +208,7 @@ int nvb_hv_kernel_in_use(nvb_handle *h, int64_t dtype, int64_t *kernel) {
         if (dtype != NVB_DTYPE_F64 && dtype != NVB_DTYPE_F32) fail(NVB_ERR_ARG, "dtype must be NVB_DTYPE_F64 or NVB_DTYPE_F32");
         if (h->device < 0) fail(NVB_ERR_STATE, "host-only handle");
         if (h->quad.ok) *kernel = 3;
+        else if (h->cubic.ok && h->cubic.prec_ok[dtype == NVB_DTYPE_F32 ? 1 : 0]) *kernel = 4;
         else if (h->slab[dtype == NVB_DTYPE_F32 ? 1 : 0].ok) *kernel = 2;
         else *kernel = 1;
     });
@@ -287,6 +294,7 @@ int nvb_set_fault_test(nvb_handle *h, int64_t mode) {
         if (!h) fail(NVB_ERR_ARG, "null handle");
         if (mode != 0 && mode != 1) fail(NVB_ERR_ARG, "fault-test mode must be 0 or 1");
         h->quad.test_nocopy = (int)mode;
+        h->cubic.test_nocopy = (int)mode;
     });
 }
 

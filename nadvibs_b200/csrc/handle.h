@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "cubic.h"
 #include "plan.h"
 #include "quad.h"
 #include "slab.h"
@@ -19,6 +20,7 @@ struct nvb_handle {
     nvb::Plan plan;
     nvb::SlabPlan slab[2];  // slab-tiled H.v plans for FP64 (0) and FP32 (1) vectors
     nvb::QuadPlan quad;     // factorised quadratic H.v plan (both precisions)
+    nvb::CubPlan cubic;     // factorised cubic H.v plan (both precisions)
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "quad.h"
 
@@ -540,7 +541,12 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                 release();
             }
             // present slow items: the Z items (y_a += c x, Z_l += z_l x), then the
-            // coefficient-only items two at a time
+            // coefficient-only items two at a time.  Z is final once the Z items are in, so
+            // y_a += X_l Z_l is applied in between the coefficient-only items: mode m at once by
+            // register shifts, every other fast mode at its own evenly spaced point, through
+            // the shared Z buffer between two consumer barriers.  (Applied in one block at the
+            // end, these steps stalled the consumers for long enough to fill the ring and idle
+            // the copies; spread out, the ring keeps streaming through each step.)
             {
                 const int nzp = s_cnt[(tp * QUAD_MAXS + a) * 2], nsp = s_cnt[(tp * QUAD_MAXS + a) * 2 + 1];
                 const T *rc = s_rec + (tp * A.nitems + s_ib[a]) * (NF + 1);
@@ -563,7 +569,42 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                     }
                     release();
                 }
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    T v = acc[r];
+                    if (r + 1 < R) v += F.em[0][r] * Z[0][r + 1];
+                    if (r >= 1) v += F.em[1][r] * Z[0][r - 1];
+                    acc[r] = v;
+                }
+                // fast mode jj >= 1: Z_jj through s_z (every consumer thread takes part)
+                auto xz = [&](auto jc) {
+                    constexpr int jj = decltype(jc)::value;
+#pragma unroll
+                    for (int r = 0; r < R; ++r) s_z[pad + r * nc + tid] = r < nv ? Z[jj][r] : (T)0;
+                    consumer_sync(nc);
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const T *p = s_z + pad + r * nc + tid;
+                        acc[r] += e1p(jj) * p[F.sh[jj]] + e1m(jj) * p[-F.sh[jj]];
+                    }
+                    consumer_sync(nc);  // s_z is rewritten next
+                };
+                int done = 1;  // fast modes applied
+                auto xz_next = [&]() {
+                    if constexpr (NF > 1) {
+                        if (done == 1) xz(std::integral_constant<int, 1>{});
+                    }
+                    if constexpr (NF > 2) {
+                        if (done == 2) xz(std::integral_constant<int, 2>{});
+                    }
+                    if constexpr (NF > 3) {
+                        if (done == 3) xz(std::integral_constant<int, 3>{});
+                    }
+                    ++done;
+                };
+                const int nco = nsp - nzp;  // the same in every consumer thread
                 for (; j + 1 < nsp; j += 2) {
+                    if (done < NF && (j - nzp) * NF >= done * nco) xz_next();
                     // two consecutive slots: the first is held (not released) while the second
                     // is awaited; the ring has at least three slots
                     const T *b0 = take();
@@ -599,27 +640,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                     }
                     release();
                 }
-            }
-            // y_a += X_l Z_l: mode m by register shifts, the other fast modes one at a time
-            // through a single shared-memory buffer
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                T v = acc[r];
-                if (r + 1 < R) v += F.em[0][r] * Z[0][r + 1];
-                if (r >= 1) v += F.em[1][r] * Z[0][r - 1];
-                acc[r] = v;
-            }
-#pragma unroll
-            for (int j = 1; j < NF; ++j) {
-#pragma unroll
-                for (int r = 0; r < R; ++r) s_z[pad + r * nc + tid] = r < nv ? Z[j][r] : (T)0;
-                consumer_sync(nc);
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const T *p = s_z + pad + r * nc + tid;
-                    acc[r] += e1p(j) * p[F.sh[j]] + e1m(j) * p[-F.sh[j]];
-                }
-                consumer_sync(nc);  // s_z is rewritten next
+                while (done < NF) xz_next();
             }
 #pragma unroll
             for (int r = 0; r < R; ++r)

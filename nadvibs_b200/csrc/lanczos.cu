@@ -176,6 +176,16 @@ void hv_any(nvb_handle *h, const void *x, void *y, int dtype, const double *scal
         if (nblocks_out) *nblocks_out = nb;
         return;
     }
+    if (h->cubic.ok && h->cubic.prec_ok[dtype == NVB_DTYPE_F32 ? 1 : 0] && aligned) {
+        int nb;
+        if (dtype == NVB_DTYPE_F64)
+            nb = cubic_launch<double>(h->cubic, (const double *)x, (double *)y, scale_dev, alpha_part, h->stream);
+        else
+            nb = cubic_launch<float>(h->cubic, (const float *)x, (float *)y, scale_dev, alpha_part, h->stream);
+        CK(cudaGetLastError());
+        if (nblocks_out) *nblocks_out = nb;
+        return;
+    }
     if (sp.ok && aligned && h->opt.hv_kernel != 1) {
         if (dtype == NVB_DTYPE_F64)
             slab_launch<double>(sp, h->plan, (const double *)x, (double *)y, scale_dev, alpha_part, h->stream);
@@ -201,6 +211,14 @@ void check_kernel_flags(nvb_handle *h) {
         if (e) {
             CK(cudaMemset(h->quad.d_err, 0, sizeof(int)));  // reported once; the handle stays usable
             fail(NVB_ERR_CUDA, "quadratic H.v: a shared-memory tile copy did not complete (kernel gave up waiting)");
+        }
+    }
+    if (h->cubic.ok && h->cubic.d_err) {
+        int e = 0;
+        CK(cudaMemcpy(&e, h->cubic.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) {
+            CK(cudaMemset(h->cubic.d_err, 0, sizeof(int)));
+            fail(NVB_ERR_CUDA, "cubic H.v: a shared-memory tile copy did not complete (kernel gave up waiting)");
         }
     }
     for (int i = 0; i < 2; ++i)

@@ -221,14 +221,16 @@ def write_inputs(directory: str, cfg: SynthConfig, niter: int | None = None, **o
 
 def random_small(seed: int, nstates: int, basis: list[int], ordr: int, dense: bool = True,
                  offdiag_even: bool = True, zero_frac: float = 0.3,
-                 offdiag_bilinear: bool = True) -> SynthConfig:
+                 offdiag_bilinear: bool = True, offdiag_max_order: int | None = None) -> SynthConfig:
     """A tiny system for edge cases: every block may carry every order (incl. off-diagonal
     constants and even powers when ``offdiag_even``), with a fraction of exact zeros.
     ``offdiag_bilinear=False`` drops the off-diagonal monomials of two or more distinct modes
-    (the vibronic-coupling form the factorised quadratic kernel accepts)."""
+    (the vibronic-coupling form the factorised quadratic kernel accepts);
+    ``offdiag_max_order=1`` keeps only constants and linear terms between different states
+    (the form the factorised cubic kernel accepts)."""
     cfg = SynthConfig(f"small{seed}", nstates, list(basis), ordr, [0.0] * nstates, {}, 30, seed)
     cfg.extra = dict(dense=dense, offdiag_even=offdiag_even, zero_frac=zero_frac,
-                     offdiag_bilinear=offdiag_bilinear)
+                     offdiag_bilinear=offdiag_bilinear, offdiag_max_order=offdiag_max_order)
     return cfg
 
 
@@ -254,6 +256,9 @@ def draw_small(cfg: SynthConfig):
                     keep[:] = False
                 if not diag and not cfg.extra.get("offdiag_bilinear", True) and d >= 2:
                     keep &= np.array([len(set(mo)) == 1 for mo in mons])
+                omax = cfg.extra.get("offdiag_max_order")
+                if not diag and omax is not None and d > omax:
+                    keep[:] = False
                 vals = np.where(keep, vals, 0.0)
                 for t, mono in enumerate(mons):
                     for m in mono:
