@@ -109,7 +109,7 @@ struct CubLayout {
     int tab, cs, sd, dig, items, seg, plist, pres, cl, cnt, rec, ring, z, total;
 };
 __host__ __device__ inline CubLayout cub_layout(int M, int S, int nmax, int m, int nF, int sstate, int eb, int nslot,
-                                                int nitems) {
+                                                int nitems, int nterms) {
     CubLayout L{};
     int o = 2 * CUB_MAXSLOT * 8 + 16;  // full / empty mbarriers, abort flag
     auto take = [&](int bytes) {
@@ -130,7 +130,9 @@ __host__ __device__ inline CubLayout cub_layout(int M, int S, int nmax, int m, i
     L.rec = take(nitems * (nF + 2) * eb);  // per item: c, e, z[nF]
     o = (o + 127) / 128 * 128;
     L.ring = take(nslot * sstate * eb);
-    L.z = take(sstate * eb);
+    // Z exchange buffer; at the start of a tile it holds the term products and their slots
+    const int zb = sstate * eb, pb = nterms * (eb + 1);
+    L.z = take(zb > pb ? zb : pb);
     L.total = o;
     return L;
 }

@@ -323,7 +323,8 @@ bool cubic_build(CubPlan &cp, const Plan &pl, const System &sys, int quirk_cubic
     for (int eb : {8, 4}) {
         const int i = eb == 8 ? 0 : 1;
         if (eb == 8 && cp.threads > 288) continue;
-        const size_t fixed = (size_t)cub_layout(M, S, nmax, m, NF, cp.sstate, eb, 0, (int)cp.items.size()).total;
+        const int nit = (int)cp.items.size(), nterm = (int)cp.tinfo.size();
+        const size_t fixed = (size_t)cub_layout(M, S, nmax, m, NF, cp.sstate, eb, 0, nit, nterm).total;
         const size_t slot = (size_t)cp.sstate * eb;
         size_t budget = 226 * 1024;
         int per = 1;
@@ -333,7 +334,7 @@ bool cubic_build(CubPlan &cp, const Plan &pl, const System &sys, int quirk_cubic
         }
         if (fixed + 3 * slot > budget) continue;
         cp.nslot[i] = (int)std::min<size_t>(CUB_MAXSLOT, (budget - fixed) / slot);
-        cp.smem[i] = (size_t)cub_layout(M, S, nmax, m, NF, cp.sstate, eb, cp.nslot[i], (int)cp.items.size()).total;
+        cp.smem[i] = (size_t)cub_layout(M, S, nmax, m, NF, cp.sstate, eb, cp.nslot[i], nit, nterm).total;
         cp.per_sm[i] = per;
         cp.prec_ok[i] = true;
     }

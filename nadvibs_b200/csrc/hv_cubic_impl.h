@@ -44,7 +44,7 @@ struct CubArgs {
     const CubItem *items;
     const int *seg;
     int *err;
-    int M, m, nmax, nv, pad, sstate, TF, ntiles, nslot, nitems;
+    int M, m, nmax, nv, pad, sstate, TF, ntiles, nslot, nitems, nterms;
     int nocopy;      // failure test: the producer issues no copy, so every consumer wait runs out
     int wait_limit;  // polls before a wait gives up
     long long dimen;
@@ -60,7 +60,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
     extern __shared__ __align__(128) unsigned char smem[];
     const int M = A.M, m = A.m, nmax = A.nmax, sst = A.sstate, TF = A.TF, NS = A.nslot, pad = A.pad;
     const int nit = A.nitems;
-    const CubLayout Lo = cub_layout(M, S, nmax, m, NF, sst, (int)sizeof(T), NS, nit);
+    const int nterm = A.nterms;
+    const CubLayout Lo = cub_layout(M, S, nmax, m, NF, sst, (int)sizeof(T), NS, nit, nterm);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
     uint64_t *empty = full + CUB_MAXSLOT;
     volatile int *abort_flag = reinterpret_cast<volatile int *>(smem + 2 * CUB_MAXSLOT * 8);
@@ -77,6 +78,9 @@ __global__ void __launch_bounds__(MAXT, MINB)
     T *s_rec = reinterpret_cast<T *>(smem + Lo.rec);
     T *s_ring = reinterpret_cast<T *>(smem + Lo.ring);  // [NS][sst]
     T *s_z = reinterpret_cast<T *>(smem + Lo.z);        // [sst] Z_f of one fast mode f >= 1
+    // at the start of a tile s_z holds the term products [nterm] and their record slots [nterm]
+    T *s_prod = s_z;
+    signed char *s_pslot = reinterpret_cast<signed char *>(s_z + nterm);
     const int tid = threadIdx.x;
     const int nc = NC > 0 ? NC : (int)blockDim.x - 32;  // consumer threads = shft(m)
     const long long N = A.dimen;
@@ -259,9 +263,19 @@ __global__ void __launch_bounds__(MAXT, MINB)
         if (tid < m) s_dig[tp * CUB_MAXSL + tid] = (tile / tsh[tid]) % snf[tid];
         consumer_sync(nc);
         const int *dig = s_dig + tp * CUB_MAXSL;
-        // every item: presence and its record for this tile
+        // every term's product for this tile, all terms in parallel (their element factors are
+        // table entries at the tile's own digits, valid whether or not the item is present);
+        // then every item's presence and record, summing its products in program order
+        for (int t = tid; t < nterm; t += nc) {
+            const CubTerm ti = A.tinfo[t];
+            T v = A.tcoef[t];
+            for (int q = 0; q < ti.nf; ++q) v *= s_tab[(ti.md[q] * CUB_ROWS + ti.rw[q]) * nmax + dig[ti.md[q]]];
+            s_prod[t] = v;
+            s_pslot[t] = ti.slot;
+        }
+        consumer_sync(nc);
         for (int i = tid; i < nit; i += nc) {
-            const CubItem ci = s_it[i];
+            const CubItem &ci = s_it[i];
             bool pres = true;
             for (int k = 0; k < ci.nsh; ++k) {
                 const int d = dig[ci.md[k]] + ci.sv[k];
@@ -271,12 +285,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
             for (int q = 0; q < NREC; ++q) rc[q] = (T)0;
             if (pres)
-                for (int t = ci.tb; t < ci.te; ++t) {
-                    const CubTerm ti = A.tinfo[t];
-                    T v = A.tcoef[t];
-                    for (int q = 0; q < ti.nf; ++q) v *= s_tab[(ti.md[q] * CUB_ROWS + ti.rw[q]) * nmax + dig[ti.md[q]]];
-                    rc[ti.slot] += v;
-                }
+                for (int t = ci.tb; t < ci.te; ++t) rc[s_pslot[t]] += s_prod[t];
             s_pres[i] = pres ? 1 : 0;
         }
         consumer_sync(nc);
@@ -303,18 +312,19 @@ __global__ void __launch_bounds__(MAXT, MINB)
         const long long tbase = (long long)tile * TF;
 #pragma unroll
         for (int a = 0; a < S; ++a) {
-            T xr[R], acc[R], Z[NF][R];
+            T acc[R], Z[NF][R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                xr[r] = acc[r] = (T)0;
+                acc[r] = (T)0;
 #pragma unroll
                 for (int j = 0; j < NF; ++j) Z[j][r] = (T)0;
             }
-            // ---- own tile x_a
+            // ---- own tile x_a (its column lives only here; the alpha partial re-reads x from L2)
             {
                 const T *rc = s_rec + s_seg[4 * a] * NREC;
                 const T *buf = take();
                 if (kNoBranch || ok) {
+                    T xr[R];
 #pragma unroll
                     for (int r = 0; r < R; ++r) xr[r] = buf[r * nc];
                     T dfast = (T)0;
@@ -491,6 +501,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
                         for (int r = 0; r < R; ++r) Z[f][r] += zf * v[r];
                     }
+                    T dq = (T)0;  // sum over f >= 1 of e cs_ff <n_f|x_f^2|n_f> (the zero shift of x_f^2)
                     auto per_mode = [&](auto fc) {
                         constexpr int f = decltype(fc)::value;
                         bool any = false;
@@ -511,8 +522,14 @@ __global__ void __launch_bounds__(MAXT, MINB)
                             T Tt[R];
                             T2f(fc, v, buf, Tt);
                             const T q = e * cff;
+                            if constexpr (f == 0) {
 #pragma unroll
-                            for (int r = 0; r < R; ++r) acc[r] += q * (Tt[r] + Df(fc, r) * v[r]);
+                                for (int r = 0; r < R; ++r) acc[r] += q * (Tt[r] + F.em[ER_D2][r] * v[r]);
+                            } else {
+#pragma unroll
+                                for (int r = 0; r < R; ++r) acc[r] += q * Tt[r];
+                                dq += q * tv(f, ER_D2);
+                            }
                         }
                     };
                     per_mode(std::integral_constant<int, 0>{});
@@ -520,6 +537,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
                     if constexpr (NF > 2) per_mode(std::integral_constant<int, 2>{});
                     if constexpr (NF > 3) per_mode(std::integral_constant<int, 3>{});
                     if constexpr (NF > 4) per_mode(std::integral_constant<int, 4>{});
+#pragma unroll
+                    for (int r = 0; r < R; ++r) acc[r] += dq * v[r];
                 }
                 release();
             }
@@ -625,9 +644,10 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
             for (int r = 0; r < R; ++r)
                 if (r < nv) {
+                    const long long o = a * N + tbase + r * nc + tid;
                     const T v = acc[r] * sc;
-                    y[a * N + tbase + r * nc + tid] = v;
-                    if (alpha_part) part += ((double)xr[r] * (double)sc) * (double)v;
+                    y[o] = v;
+                    if (alpha_part) part += ((double)x[o] * (double)sc) * (double)v;
                 }
         }
     }
@@ -666,6 +686,7 @@ CubArgs<T> cub_args(const CubPlan &cp) {
     a.TF = cp.TF;
     a.ntiles = cp.ntiles;
     a.nitems = (int)cp.items.size();
+    a.nterms = (int)cp.tinfo.size();
     a.dimen = cp.dimen;
     if constexpr (sizeof(T) == 8) {
         a.blk = (const T *)cp.d_blk;
