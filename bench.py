@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient (grad/fwd) measurement")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the mixed-vs-FP64 Ritz comparison")
-    ap.add_argument("--no-fma", action="store_true", help="skip the measured FMA ceilings")
+    ap.add_argument("--no-fma", action="store_true", help="skip the measured FMA and tile-stream ceilings")
     ap.add_argument("--no-config5", action="store_true",
                     help="skip the short literal-size run of the cubic system (config 5)")
     ap.add_argument("--no-reorth", action="store_true",
@@ -197,7 +197,8 @@ def run_ours(args, rank, world, dev):
         hv_ms, it_ms, n = h.timing()
         results[prec] = dict(ms=ms_max, hv_ms_per=hv_ms / max(n, 1), it_ms_per=it_ms / max(n, 1),
                              clocks=clk.summary(), bytes_hv=2 * N * eb, alpha=a[-3:].tolist(),
-                             beta=b[-3:].tolist(), launches=4 * args.steps, kernel=kname)
+                             beta=b[-3:].tolist(), launches=4 * args.steps, kernel=kname,
+                             stream=h.hv_tile_stream(L.DTYPE_F64 if prec == "fp64" else L.DTYPE_F32))
         h.close()
         torch.cuda.empty_cache()
     # end-to-end through the public API with host buffers: create from files (host input),
@@ -388,6 +389,20 @@ def grad_timing(dev: int):
             "grad_over_fwd": g / f}
 
 
+def tile_stream(stream: dict | None, hv_ms: float, seconds: float = 1.0):
+    """The factorised H.v's neighbour-tile stream (bytes copied L2 -> shared memory per product)
+    against its measured ceiling: whole tiles of the same size streamed into a ring of the same
+    slots and CTAs per multiprocessor with no arithmetic (nvb_measure_tile_stream)."""
+    from nadvibs_b200 import _lib as L
+    if not stream or stream["bytes_per_hv"] <= 0:
+        return None
+    ceiling = L.measure_tile_stream(stream["tile_bytes"], stream["slots"], stream["ctas_per_sm"], seconds)
+    achieved = stream["bytes_per_hv"] / (hv_ms / 1e3)
+    return {"bytes_per_hv": stream["bytes_per_hv"], "tile_bytes": stream["tile_bytes"], "slots": stream["slots"],
+            "ctas_per_sm": stream["ctas_per_sm"], "achieved_gbs": achieved / 1e9, "ceiling_gbs": ceiling / 1e9,
+            "frac": achieved / ceiling, "ceiling_kind": "measured (nvb_measure_tile_stream)"}
+
+
 def large_cubic(dev: int, iters: int = 4, warm: int = 2, grad_iters: int = 60, budget: float = 150e9,
                 with_grad: bool = True):
     """Config 5, ordr 3 (cubic terms N(0,10 cm^-1)), 3 states, 10 modes, FP32 vectors / FP64
@@ -421,12 +436,18 @@ def large_cubic(dev: int, iters: int = 4, warm: int = 2, grad_iters: int = 60, b
         h.seed()
         h.lanczos(warm)
         torch.cuda.synchronize()
+        h.set_timing(True)
         t0 = time.perf_counter()
         h.lanczos(iters)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        out["literal"] = {"basis": list(cfg.basis), "elements": int(np.prod(cfg.basis)) * cfg.nstates,
+        hv_ms, _, nt = h.timing()
+        hv_ms /= max(nt, 1)
+        n_el = int(np.prod(cfg.basis)) * cfg.nstates
+        out["literal"] = {"basis": list(cfg.basis), "elements": n_el,
                           "kernel": h.hv_kernel(L.DTYPE_F32), "iter_per_s": iters / dt, "ms_per_iter": 1e3 * dt / iters,
+                          "hv_ms": hv_ms, "hv_gbs": 2 * n_el * 4 / (hv_ms / 1e3) / 1e9,
+                          "tile_stream": tile_stream(h.hv_tile_stream(L.DTYPE_F32), hv_ms),
                           "device_gb_in_use_after_create": (total - free) / 1e9, "iterations_timed": iters}
     finally:
         h.close()
@@ -607,6 +628,11 @@ def main():
             line["alu"]["frac_of_measured_fp64"] = line["alu"]["achieved_tflops"] / (f64 / 1e12)
             if "mixed_achieved_tflops" in line["alu"]:
                 line["alu"]["mixed_frac_of_measured_fp32"] = line["alu"]["mixed_achieved_tflops"] / (f32 / 1e12)
+            # the factorised kernel's own bound: its neighbour-tile stream against the measured
+            # ceiling of that stream
+            line["roofline"]["tile_stream"] = tile_stream(r.get("stream"), r["hv_ms_per"])
+            if "mixed" in line:
+                line["mixed"]["tile_stream"] = tile_stream(res["mixed"].get("stream"), res["mixed"]["hv_ms_per"])
     if rank == 0 and not args.no_grad:
         line["grad"] = grad_timing(local)
     if rank == 0 and args.config5:

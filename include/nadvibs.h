@@ -356,6 +356,23 @@ int nvb_dot_noalloc(const void *a, double sa, const void *b, double sb, int64_t 
  * NVB_DTYPE_F32.  The arithmetic ceiling the H.v kernels' flops are compared with. */
 int nvb_measure_fma(int64_t dtype, double seconds, double *flops_per_s);
 
+/* Measured rate (bytes/s) at which whole tiles of tile_bytes can be streamed from L2 into
+ * shared memory on the current device by the tiled H.v kernels' data path (no reference
+ * counterpart): ctas_per_sm CTAs per multiprocessor, each a producer warp issuing TMA bulk
+ * copies of pseudo-random tiles of a 64 MB buffer into a ring of `slots` slots and 9 consumer
+ * warps that read each slot before releasing it, no arithmetic, about `seconds` of device time
+ * timed with CUDA events.  The ceiling of the factorised kernels' neighbour-tile stream. */
+int nvb_measure_tile_stream(int64_t tile_bytes, int64_t slots, int64_t ctas_per_sm, double seconds,
+                            double *bytes_per_s);
+
+/* The neighbour-tile stream of a factorised H.v (quadratic or cubic kernel) for vectors of
+ * dtype: bytes copied from L2 into shared memory per product (every item whose neighbour tile
+ * lies inside the basis, once per tile), the tile size, and the ring's slots and CTAs per
+ * multiprocessor (after a first product; 1 before).  All zero when the dtype's products use the
+ * slab or gather kernel.  No reference counterpart. */
+int nvb_hv_tile_stream(nvb_handle *h, int64_t dtype, double *bytes_per_hv, int64_t *tile_bytes, int64_t *slots,
+                       int64_t *ctas_per_sm);
+
 /* Per-phase device timing of nvb_lanczos (the reference writes per-phase wall times to
  * output.dat, Source/top.f90:663-667,814-817,834-841): when enabled, CUDA events on the
  * handle's stream bracket the H.v launch and the whole iteration; nvb_get_timing returns

@@ -57,6 +57,8 @@ _SIGS = {
     "nvb_reorth_log": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_reorth_omega": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_measure_fma": [C.c_int64, C.c_double, C.c_void_p],
+    "nvb_measure_tile_stream": [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_void_p],
+    "nvb_hv_tile_stream": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "nvb_write_seed_report": [C.c_void_p, C.c_char_p],
     "nvb_set_fault_test": [C.c_void_p, C.c_int64],
     "nvb_set_displaced_seed": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
@@ -129,6 +131,13 @@ def measure_fma(dtype: int, seconds: float = 2.0) -> float:
     """nvb_measure_fma: FMA throughput of the current device (flop/s, 2 per FMA)."""
     r = C.c_double()
     check(lib().nvb_measure_fma(dtype, seconds, C.byref(r)))
+    return r.value
+
+
+def measure_tile_stream(tile_bytes: int, slots: int = 8, ctas_per_sm: int = 1, seconds: float = 1.0) -> float:
+    """nvb_measure_tile_stream: bytes/s of whole tiles streamed from L2 into a shared-memory ring."""
+    r = C.c_double()
+    check(lib().nvb_measure_tile_stream(tile_bytes, slots, ctas_per_sm, seconds, C.byref(r)))
     return r.value
 
 
@@ -211,6 +220,14 @@ class Handle:
         v = [C.c_int64() for _ in range(6)]
         check(lib().nvb_get_sizes(self.ptr, *[C.byref(x) for x in v]))
         return dict(zip(("dimen", "nstates", "nmodes", "nterms", "npot", "iters"), [x.value for x in v]))
+
+    def hv_tile_stream(self, dtype: int = DTYPE_F64) -> dict:
+        """nvb_hv_tile_stream: the factorised H.v's neighbour-tile stream (bytes per product,
+        tile bytes, ring slots, CTAs per multiprocessor); zeros for the slab / gather kernels."""
+        b = C.c_double()
+        v = [C.c_int64() for _ in range(3)]
+        check(lib().nvb_hv_tile_stream(self.ptr, dtype, C.byref(b), *[C.byref(x) for x in v]))
+        return {"bytes_per_hv": b.value, "tile_bytes": v[0].value, "slots": v[1].value, "ctas_per_sm": v[2].value}
 
     def hv_kernel(self, dtype: int = DTYPE_F64) -> str:
         """Name of the H.v kernel products of this dtype run: gather, slab, quad or cubic."""

@@ -1,4 +1,5 @@
 // extern "C" entry points of libnadvibs_gpu.so (declared in include/nadvibs.h).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -201,6 +202,48 @@ int nvb_destroy(nvb_handle *h) {
 }
 
 const char *nvb_last_error(void) { return g_err.c_str(); }
+
+int nvb_hv_tile_stream(nvb_handle *h, int64_t dtype, double *bytes_per_hv, int64_t *tile_bytes, int64_t *slots,
+                       int64_t *ctas_per_sm) {
+    return guarded([&] {
+        if (!h || !bytes_per_hv || !tile_bytes || !slots || !ctas_per_sm) fail(NVB_ERR_ARG, "null argument");
+        if (dtype != NVB_DTYPE_F64 && dtype != NVB_DTYPE_F32) fail(NVB_ERR_ARG, "dtype must be NVB_DTYPE_F64 or NVB_DTYPE_F32");
+        if (h->device < 0) fail(NVB_ERR_STATE, "host-only handle");
+        const int idx = dtype == NVB_DTYPE_F32 ? 1 : 0, eb = idx ? 4 : 8;
+        *bytes_per_hv = 0.0;
+        *tile_bytes = *slots = *ctas_per_sm = 0;
+        int nsm = 0;
+        CKA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+        // fraction of tiles whose neighbour along slow mode k at shift s lies inside the basis
+        auto inside = [](int nf, int s) { return (double)std::max(nf - std::abs(s), 0) / (double)nf; };
+        if (h->quad.ok) {
+            const nvb::QuadPlan &q = h->quad;
+            double items = 0.0;
+            for (const nvb::QuadItem &it : q.items) {
+                double f = 1.0;
+                if (it.kind != nvb::QI_OWN) f *= inside(q.slow_nfunc[it.k], it.sk);
+                if (it.kind == nvb::QI_PAIR) f *= inside(q.slow_nfunc[it.l], it.sl);
+                items += f;
+            }
+            *bytes_per_hv = items * (double)q.ntiles * (double)q.TF * eb;
+            *tile_bytes = (int64_t)q.TF * eb;
+            *slots = q.nslot[idx];
+            *ctas_per_sm = q.grid[idx] > 0 ? std::max<int64_t>(1, q.grid[idx] / nsm) : 1;
+        } else if (h->cubic.ok && h->cubic.prec_ok[idx]) {
+            const nvb::CubPlan &c = h->cubic;
+            double items = 0.0;
+            for (const nvb::CubItem &it : c.items) {
+                double f = 1.0;
+                for (int k = 0; k < it.nsh; ++k) f *= inside(c.slow_nfunc[it.md[k]], it.sv[k]);
+                items += f;
+            }
+            *bytes_per_hv = items * (double)c.ntiles * (double)c.TF * eb;
+            *tile_bytes = (int64_t)c.TF * eb;
+            *slots = c.nslot[idx];
+            *ctas_per_sm = c.grid[idx] > 0 ? std::max<int64_t>(1, c.grid[idx] / nsm) : c.per_sm[idx];
+        }
+    });
+}
 
 int nvb_hv_kernel_in_use(nvb_handle *h, int64_t dtype, int64_t *kernel) {
     return guarded([&] {

@@ -59,6 +59,21 @@ module nadvibs_gpu
       real(c_double), value :: seconds
       real(c_double), intent(out) :: flops_per_s
     end function
+    integer(c_int) function nvb_measure_tile_stream(tile_bytes, slots, ctas_per_sm, seconds, bytes_per_s) &
+        bind(C, name="nvb_measure_tile_stream")
+      import :: c_int, c_int64_t, c_double
+      integer(c_int64_t), value :: tile_bytes, slots, ctas_per_sm
+      real(c_double), value :: seconds
+      real(c_double), intent(out) :: bytes_per_s
+    end function
+    integer(c_int) function nvb_hv_tile_stream(h, dtype, bytes_per_hv, tile_bytes, slots, ctas_per_sm) &
+        bind(C, name="nvb_hv_tile_stream")
+      import :: c_int, c_int64_t, c_double, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int64_t), value :: dtype
+      real(c_double), intent(out) :: bytes_per_hv
+      integer(c_int64_t), intent(out) :: tile_bytes, slots, ctas_per_sm
+    end function
     integer(c_int) function nvb_write_seed_report(h, path) bind(C, name="nvb_write_seed_report")
       import :: c_int, c_char, c_ptr
       type(c_ptr), value :: h
