@@ -123,9 +123,9 @@ __host__ __device__ inline CubLayout cub_layout(int M, int S, int nmax, int m, i
     L.dig = take(2 * CUB_MAXSL * 4);       // per tile parity: slow digits
     L.items = take(nitems * (int)sizeof(CubItem));
     L.seg = take((4 * CUB_MAXS + 1) * 4);
-    L.plist = take(2 * (nitems + 1) * 4);  // producer: per tile parity, count and present items
-    L.pres = take(nitems * 4);             // consumers: presence of every item in the tile
-    L.cl = take(nitems * 4);               // consumers: present items of each target, in order
+    L.plist = take(2 * (nitems + 1) * 8);  // producer: per tile parity, count and present items' source offsets
+    L.pres = take(nitems);                 // consumers: presence of every item in the tile
+    L.cl = take(nitems * 2);               // consumers: present items of each target, in order (< 4096)
     L.cnt = take(CUB_MAXS * 4 * 4);        // per target: Q, Z, C items present
     L.rec = take(nitems * (nF + 2) * eb);  // per item: c, e, z[nF]
     o = (o + 127) / 128 * 128;

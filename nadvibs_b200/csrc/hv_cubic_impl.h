@@ -71,9 +71,9 @@ __global__ void __launch_bounds__(MAXT, MINB)
     int *s_dig = reinterpret_cast<int *>(smem + Lo.dig);  // [2][MAXSL] slow digits of a tile
     CubItem *s_it = reinterpret_cast<CubItem *>(smem + Lo.items);
     int *s_seg = reinterpret_cast<int *>(smem + Lo.seg);
-    int *s_pl = reinterpret_cast<int *>(smem + Lo.plist);
-    int *s_pres = reinterpret_cast<int *>(smem + Lo.pres);
-    int *s_cl = reinterpret_cast<int *>(smem + Lo.cl);
+    long long *s_pl = reinterpret_cast<long long *>(smem + Lo.plist);
+    unsigned char *s_pres = smem + Lo.pres;
+    short *s_cl = reinterpret_cast<short *>(smem + Lo.cl);
     int *s_cnt = reinterpret_cast<int *>(smem + Lo.cnt);
     T *s_rec = reinterpret_cast<T *>(smem + Lo.rec);
     T *s_ring = reinterpret_cast<T *>(smem + Lo.ring);  // [NS][sst]
@@ -114,13 +114,15 @@ __global__ void __launch_bounds__(MAXT, MINB)
 
     if (tid >= nc) {
         // ---------------- producer ----------------
-        // The warp lists each tile's present items (ballot per 32 items, compacted into s_pl[q]
-        // for tile parity q, count first) one tile ahead; lane 0 issues the tile's copies in
-        // consumption order, each after its slot was released.
+        // The warp lists each tile's present items one tile ahead (ballot per 32 items, compacted
+        // into s_pl[q] for tile parity q: the count, then each item's source offset in x relative
+        // to the tile); lane 0 issues the tile's copies in consumption order, each after its slot
+        // was released, reading the next offset before it waits (the producer lane is on the
+        // critical path).
         const int lane = tid - nc;
         const unsigned bytes = (unsigned)TF * (unsigned)sizeof(T);
         auto list = [&](int tile, int q) {
-            int *pl = s_pl + q * (nit + 1);
+            long long *pl = s_pl + q * (nit + 1);
             int base = 0;
             for (int i0 = 0; i0 < nit; i0 += 32) {
                 const int it = i0 + lane;
@@ -135,7 +137,10 @@ __global__ void __launch_bounds__(MAXT, MINB)
                     }
                 }
                 const unsigned bal = __ballot_sync(0xffffffffu, ok);
-                if (ok) pl[1 + base + __popc(bal & ((1u << lane) - 1u))] = it;
+                if (ok) {
+                    const CubItem &ci = s_it[it];
+                    pl[1 + base + __popc(bal & ((1u << lane) - 1u))] = (long long)ci.b * N + (long long)ci.tshift * TF;
+                }
                 base += __popc(bal);
             }
             if (lane == 0) pl[0] = base;
@@ -149,18 +154,19 @@ __global__ void __launch_bounds__(MAXT, MINB)
         int q = 0;
         for (int tile = blockIdx.x; tile < A.ntiles && !stop; tile += gridDim.x, q ^= 1) {
             if (tile + (int)gridDim.x < A.ntiles) list(tile + gridDim.x, q ^ 1);
-            const int *pl = s_pl + q * (nit + 1);
-            const int cnt = pl[0];
+            const long long *pl = s_pl + q * (nit + 1);
+            const int cnt = (int)pl[0];
             if (lane == 0) {
-                const long long tb = (long long)tile * TF;
+                const T *xt = x + (long long)tile * TF;
+                long long nxt = cnt > 0 ? pl[1] : 0;
                 for (int i = 0; i < cnt && !stop; ++i) {
-                    const CubItem &ci = s_it[pl[1 + i]];
+                    const long long off = nxt;
+                    if (i + 1 < cnt) nxt = pl[2 + i];
                     // a consumer whose wait gave up never releases its slot, so no slot with a
                     // copy in flight is reissued: the producer's wait for it runs out and it stops
                     if (mbar_wait(&empty[slot], ph ^ 1u, abort_flag, A.wait_limit)) {
                         mbar_expect_tx(&full[slot], bytes);
-                        bulk_g2s(s_ring + slot * sst + pad, x + ci.b * N + tb + (long long)ci.tshift * TF, bytes,
-                                 &full[slot]);
+                        bulk_g2s(s_ring + slot * sst + pad, xt + off, bytes, &full[slot]);
                         ++issued;
                     } else {
                         stop = 1;
@@ -297,7 +303,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
                 const int i = i0 + lane;
                 const bool p = i < end && s_pres[i] != 0;
                 const unsigned bal = __ballot_sync(0xffffffffu, p);
-                if (p) s_cl[q0 + base + __popc(bal & ((1u << lane) - 1u))] = i;
+                if (p) s_cl[q0 + base + __popc(bal & ((1u << lane) - 1u))] = (short)i;
                 base += __popc(bal);
                 nq += __popc(__ballot_sync(0xffffffffu, p && i < z0));
                 nz += __popc(__ballot_sync(0xffffffffu, p && i >= z0 && i < c0));
@@ -602,7 +608,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
             };
             // ---- coefficient-only items, two at a time
             {
-                const int *cl = s_cl + qbase + nq + nz;
+                const short *cl = s_cl + qbase + nq + nz;
                 int j = 0;
                 for (; j + 1 < ncc; j += 2) {
                     if (done < NF && j * NF >= done * ncc) xz_next();

@@ -187,17 +187,19 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
     if (tid >= nc) {
         // ---------------- producer ----------------
         // One tile ahead of the copies the warp lists the tile's present items (ballot per 32
-        // items, compacted into s_pl[q] for tile parity q, count first); lane 0 then issues
-        // the tile's copies from the list in consumption order, each after its slot was
-        // released.  (Listing ahead keeps the ballots out of the gap between two tiles' copies;
-        // one issuing lane keeps the copies in the order the consumers take them, which
-        // measured faster than one lane per slot.)
+        // items, compacted into s_pl[q] for tile parity q: the count, then each item's source
+        // offset in x relative to the tile); lane 0 then issues the tile's copies from the list
+        // in consumption order, each after its slot was released, reading the next offset
+        // before it waits.  (The producer lane is on the critical path: listing ahead keeps the
+        // ballots out of the gap between two tiles' copies, and the precomputed offsets keep
+        // the item records and their address arithmetic out of the issue loop; one issuing lane
+        // keeps the copies in the order the consumers take them.)
         const int lane = tid - nc;
         const unsigned bytes = (unsigned)TF * (unsigned)sizeof(T);
         const int nit = s_ib[S];
-        int *s_pl = reinterpret_cast<int *>(smem + Lo.plist);  // [2][nitems + 1]
+        long long *s_pl = reinterpret_cast<long long *>(smem + Lo.plist);  // [2][nitems + 1]
         auto list = [&](int tile, int q) {
-            int *pl = s_pl + q * (nit + 1);
+            long long *pl = s_pl + q * (nit + 1);
             int base = 0;
             for (int i0 = 0; i0 < nit; i0 += 32) {
                 const int it = i0 + lane;
@@ -215,7 +217,11 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                     }
                 }
                 const unsigned bal = __ballot_sync(0xffffffffu, ok);
-                if (ok) pl[1 + base + __popc(bal & ((1u << lane) - 1u))] = it;
+                if (ok) {
+                    const QuadItem &qi = s_it[it];
+                    pl[1 + base + __popc(bal & ((1u << lane) - 1u))] =
+                        (long long)qi.b * N + (long long)qi.tshift * TF;
+                }
                 base += __popc(bal);
             }
             if (lane == 0) pl[0] = base;
@@ -229,12 +235,14 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
         int q = 0;
         for (int tile = blockIdx.x; tile < A.ntiles && !stop; tile += gridDim.x, q ^= 1) {
             if (tile + (int)gridDim.x < A.ntiles) list(tile + gridDim.x, q ^ 1);
-            const int *pl = s_pl + q * (nit + 1);
-            const int cnt = pl[0];
+            const long long *pl = s_pl + q * (nit + 1);
+            const int cnt = (int)pl[0];
             if (lane == 0) {
-                const long long tb = (long long)tile * TF;
+                const T *xt = x + (long long)tile * TF;
+                long long nxt = cnt > 0 ? pl[1] : 0;
                 for (int i = 0; i < cnt && !stop; ++i) {
-                    const QuadItem qi = s_it[pl[1 + i]];
+                    const long long off = nxt;
+                    if (i + 1 < cnt) nxt = pl[2 + i];
                     // No slot whose copy may still be in flight is ever free here: a consumer
                     // whose wait gave up does not release its slot, so the producer's wait for
                     // that slot runs out (or sees the abort flag) and it stops.  (Reading the
@@ -242,8 +250,7 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                     // producer lane is on the critical path.)
                     if (mbar_wait(&empty[slot], ph ^ 1u, abort_flag, A.wait_limit)) {
                         mbar_expect_tx(&full[slot], bytes);
-                        bulk_g2s(s_ring + slot * sst + pad, x + qi.b * N + tb + (long long)qi.tshift * TF, bytes,
-                                 &full[slot]);
+                        bulk_g2s(s_ring + slot * sst + pad, xt + off, bytes, &full[slot]);
                         ++issued;
                     } else {
                         stop = 1;

@@ -119,7 +119,7 @@ __host__ __device__ inline QuadLayout quad_layout(int M, int S, int nmax, int m,
     L.dt = take(2 * (S * S + 1) * eb);
     L.items = take(nitems * (int)sizeof(QuadItem) + (3 * QUAD_MAXS + 1) * 4);
     L.cnt = take(2 * QUAD_MAXS * 2 * 4);            // per tile parity and target: Z items, slow items present
-    L.plist = take(2 * (nitems + 1) * 4);           // producer: per tile parity, count and present items
+    L.plist = take(2 * (nitems + 1) * 8);           // producer: per tile parity, count and the present items' source offsets
     L.rec = take(2 * nitems * (nF + 1) * eb);       // per tile parity: c, z[nF] of the present slow items
     o = (o + 127) / 128 * 128;
     L.ring = take(nslot * sstate * eb);
