@@ -227,9 +227,14 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
             if (lane == 0) pl[0] = base;
             __syncwarp();
         };
-        int slot = 0;
+        // Issuing lanes: lane L < IL issues the items with global index g = L, L + IL, ... into
+        // slot g % NS (phase (g / NS) & 1), so every slot is still filled in item order and
+        // guarded by its own empty / full phases.  FP32 streams twice as many (half-size) tiles
+        // per byte and issues from two lanes (5 % faster on config 2); FP64 from one.
+        constexpr int IL = sizeof(T) == 4 ? 2 : 1;
+        int slot = lane % NS;
         unsigned ph = 0;
-        long long issued = 0;
+        long long issued = 0, g0 = 0;  // g0: global index of the tile's first item
         int stop = A.nocopy;
         if (blockIdx.x < A.ntiles) list(blockIdx.x, 0);
         int q = 0;
@@ -237,17 +242,19 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
             if (tile + (int)gridDim.x < A.ntiles) list(tile + gridDim.x, q ^ 1);
             const long long *pl = s_pl + q * (nit + 1);
             const int cnt = (int)pl[0];
-            if (lane == 0) {
+            if (lane < IL) {
                 const T *xt = x + (long long)tile * TF;
-                long long nxt = cnt > 0 ? pl[1] : 0;
-                for (int i = 0; i < cnt && !stop; ++i) {
+                int i = 0;
+                if constexpr (IL > 1) i = (int)(((lane - g0) % IL + IL) % IL);
+                long long nxt = i < cnt ? pl[1 + i] : 0;
+                for (; i < cnt && !stop; i += IL) {
                     const long long off = nxt;
-                    if (i + 1 < cnt) nxt = pl[2 + i];
+                    if (i + IL < cnt) nxt = pl[1 + i + IL];
                     // No slot whose copy may still be in flight is ever free here: a consumer
                     // whose wait gave up does not release its slot, so the producer's wait for
                     // that slot runs out (or sees the abort flag) and it stops.  (Reading the
                     // abort flag before every copy as well costs ~20 % of the kernel time: the
-                    // producer lane is on the critical path.)
+                    // producer lanes are on the critical path.)
                     if (mbar_wait(&empty[slot], ph ^ 1u, abort_flag, A.wait_limit)) {
                         mbar_expect_tx(&full[slot], bytes);
                         bulk_g2s(s_ring + slot * sst + pad, xt + off, bytes, &full[slot]);
@@ -255,21 +262,36 @@ __global__ void __launch_bounds__(QUAD_MAXTH, sizeof(T) == 4 ? 2 : 1)
                     } else {
                         stop = 1;
                     }
-                    if (++slot == NS) {
-                        slot = 0;
-                        ph ^= 1u;
+                    if constexpr (IL == 1) {
+                        if (++slot == NS) {
+                            slot = 0;
+                            ph ^= 1u;
+                        }
+                    } else {
+                        slot += IL;
+                        if (slot >= NS) {
+                            slot -= NS;
+                            ph ^= 1u;
+                        }
                     }
                 }
             }
-            stop = __shfl_sync(0xffffffffu, stop, 0);
+            if constexpr (IL > 1) {
+                g0 += cnt;
+                stop = __any_sync(0xffffffffu, stop);
+            } else {
+                stop = __shfl_sync(0xffffffffu, stop, 0);
+            }
         }
-        if (lane == 0 && stop) {
-            // the copies still in flight complete on their full barriers: wait for them
-            // (bounded) before the CTA leaves
-            const long long n = issued < NS ? issued : NS;
-            for (long long i = issued - n; i < issued; ++i) {
-                const int s2 = (int)(i % NS);
-                const unsigned p = (unsigned)((i / NS) & 1);
+        if (lane < IL && stop) {
+            // each issuing lane waits (bounded) for its own copies still in flight (its k-th
+            // copy went to slot (L + IL k) % NS) before the CTA leaves
+            const long long per = (NS + IL - 1) / IL;
+            const long long n = issued < per ? issued : per;
+            for (long long k = issued - n; k < issued; ++k) {
+                const long long g = lane + (long long)IL * k;
+                const int s2 = (int)(g % NS);
+                const unsigned p = (unsigned)((g / NS) & 1);
                 for (int w = 0; w < WAIT_LIMIT && !mbar_try(&full[s2], p); ++w) {
                 }
             }

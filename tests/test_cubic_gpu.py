@@ -111,3 +111,42 @@ def test_hv_cubic_lanczos_matches_oracle():
     ao, bo, _, _ = S.lanczos(20)
     np.testing.assert_allclose(a, ao, rtol=1e-10, atol=0)
     np.testing.assert_allclose(b, bo[:21], rtol=1e-10, atol=0)
+
+
+@pytest.mark.parametrize("basis", [[4, 4, 6, 5, 8, 8, 6, 6, 4, 4], None])
+def test_hv_cubic_benchmark_system_rows_and_symmetry(basis):
+    """Config 5's Hamiltonian through the cubic kernel in FP32, on a reduced basis and at the
+    literal size (2.97e9 elements, 11.9 GB per vector): oracle rows at 1000 random positions
+    (plus the first and last rows) of H x for the same FP32-rounded x, and <u,Hx> = <Hu,x>
+    over the whole vector."""
+    cfg = synth.config(5)
+    if basis is not None:
+        cfg.basis = basis
+    om, cc, pot = synth.draw(cfg)
+    S = O.system_from_arrays(cfg.basis, cfg.nstates, cfg.ordr, om, cc, pot)
+    N = S.dimen
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.randn(S.ntotal, generator=g, device="cuda", dtype=torch.float32)
+    u = torch.randn(S.ntotal, generator=g, device="cuda", dtype=torch.float32)
+    with L.Handle.from_arrays(_params(cfg), om, cc, synth.flatten_pot(pot), precision=L.NVB_MIXED) as h:
+        assert h.hv_kernel(L.DTYPE_F32) == "cubic"
+        h.set_stream(torch.cuda.current_stream().cuda_stream)
+        y = torch.empty_like(x)
+        h.hv_ptr(x.data_ptr(), y.data_ptr(), L.DTYPE_F32)
+        hu = torch.empty_like(u)
+        h.hv_ptr(u.data_ptr(), hu.data_ptr(), L.DTYPE_F32)
+        torch.cuda.synchronize()
+    def dot(a, b):  # FP64 dot product in chunks (one torch.dot takes at most 2^31 elements)
+        c = 1 << 28
+        return sum(torch.dot(a[i:i + c].double(), b[i:i + c].double()).item() for i in range(0, a.numel(), c))
+
+    lhs, rhs = dot(u, y), dot(hu, x)
+    assert abs(lhs - rhs) <= 1e-5 * np.sqrt(dot(y, y) * dot(u, u))
+    del hu, u
+    rng = np.random.default_rng(5)
+    rows = np.concatenate([[0, N - 1], rng.integers(0, N, size=1000)])
+    xh = x.cpu().numpy().astype(np.float64)
+    yr = S.hv_rows(xh, rows)
+    idx = torch.from_numpy(rows).to("cuda")
+    yg = y.view(cfg.nstates, N)[:, idx].double().cpu().numpy().T
+    assert np.abs(yg - yr).max() <= TOL32 * np.abs(yr).max()
