@@ -327,6 +327,345 @@ __global__ void k_gram_reduce(const double *__restrict__ part, int ng, int nout,
     if (lane == 0) out[o] = accumulate ? out[o] + s : s;
 }
 
+// ---- ordr 3: P_m for every monomial of degree <= 3 is an entry of G = A^T B with
+//   A = [u_a, X_k u_a, x_k^2 u_a],
+//   B = [v_b, X_k v_b, x_k^2 v_b, (n_k + 1/2) v_b, x_k^3 v_b, X_l X_m v_b (l < m)]
+// (x_k^p with the analytic truncated elements H.v applies, the cubic quirk included; all
+// operators symmetric and operators on different modes commuting):
+//   x_k: <u_a, X_k v_b>   x_k^2: <u_a, x_k^2 v_b>   x_k^3: <u_a, x_k^3 v_b>
+//   x_k x_l: <X_k u_a, X_l v_b>   x_k^2 x_l: <x_k^2 u_a, X_l v_b>
+//   x_k x_l x_m (k < l < m): <X_k u_a, X_l X_m v_b>,   C = <u_a, v_b>,   K_k = sum_a <u_a, (n_k+1/2) v_a>.
+// Only those entries are formed: a task list of (A column, up to 4 B columns).  Per tile of
+// G3_TR = 32 rows the columns are expanded into shared memory (digits decoded once per row;
+// a warp per (state, mode) or (state, pair of modes) family and a lane per row, so each gather
+// reads consecutive rows), then every thread accumulates its tasks over the tile's rows.
+// Block partials are summed in a fixed order.
+
+constexpr int G3_TR = 32;
+constexpr int G3_THREADS = 512;
+struct G3Task {
+    short ia, nq;
+    short jb[4];
+};
+
+template <typename T, int TPT>
+__global__ void __launch_bounds__(G3_THREADS, 1) k_adj_gram3(const T *__restrict__ u, const T *__restrict__ v,
+                                                          const double *__restrict__ etab, int nmax,
+                                                          const int *__restrict__ nfunc,
+                                                          const long long *__restrict__ shft, int M, int S,
+                                                          long long dimen, const G3Task *__restrict__ tasks,
+                                                          int ntask, int accumulate, double *__restrict__ part) {
+    extern __shared__ double sm[];
+    const int MS = M * S, P2 = M * (M - 1) / 2, nA = S + 2 * MS, nB = S + 4 * MS + P2 * S;
+    const int nB1 = nB + 1;  // column nB stays zero: the padding of tasks with fewer than 4 outputs
+    const int nout = 4 * ntask;
+    double *sA = sm, *sB = sm + G3_TR * nA;             // [row][col]
+    double *stab = sB + G3_TR * nB1;                     // element rows E1, E2, D2, E31, E33 [nmax]
+    long long *ssh = reinterpret_cast<long long *>(stab + 5 * nmax);  // [M] strides
+    int *sdig = reinterpret_cast<int *>(ssh + M);        // [row][mode]
+    int *spair = sdig + G3_TR * M;                       // pair p: l | m << 8
+    int *snf = spair + P2;                               // [M] nfunc
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const bool small = dimen <= 0xFFFFFFFFll;
+    for (int i = tid; i < nmax; i += nth) {
+        stab[0 * nmax + i] = etab[(0 * ETAB_J + 1) * nmax + i];  // <n|x|n+1>
+        stab[1 * nmax + i] = etab[(1 * ETAB_J + 2) * nmax + i];  // <n|x^2|n+2>
+        stab[2 * nmax + i] = etab[(1 * ETAB_J + 0) * nmax + i];  // <n|x^2|n>
+        stab[3 * nmax + i] = etab[(2 * ETAB_J + 1) * nmax + i];  // <n|x^3|n+1>
+        stab[4 * nmax + i] = etab[(2 * ETAB_J + 3) * nmax + i];  // <n|x^3|n+3>
+    }
+    for (int k = tid; k < M; k += nth) {
+        ssh[k] = shft[k];
+        snf[k] = nfunc[k];
+    }
+    for (int e = tid; e < G3_TR; e += nth) sB[e * nB1 + nB] = 0.0;
+    if (tid == 0) {
+        int q = 0;
+        for (int l = 0; l < M; ++l)
+            for (int m = l + 1; m < M; ++m) spair[q++] = l | (m << 8);
+    }
+    const double *E1 = stab, *E2 = stab + nmax, *D2 = stab + 2 * nmax, *E31 = stab + 3 * nmax, *E33 = stab + 4 * nmax;
+    // this thread's tasks: A column and 4 B columns (padded with the zero column)
+    int ia[TPT], jb[TPT][4], nq[TPT];
+    double acc[TPT][4];
+#pragma unroll
+    for (int j = 0; j < TPT; ++j) {
+        const int t = tid + j * nth;
+        G3Task tk = t < ntask ? tasks[t] : G3Task{0, 0, {0, 0, 0, 0}};
+        ia[j] = tk.ia;
+        nq[j] = tk.nq;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            jb[j][q] = q < tk.nq ? tk.jb[q] : nB;
+            acc[j][q] = 0.0;
+        }
+    }
+    __syncthreads();
+    static_assert(G3_TR == 32, "one lane per row of the tile");
+    const int lane = tid & 31, wid = tid >> 5, nwarp = nth >> 5;
+    for (long long t0 = (long long)blockIdx.x * G3_TR; t0 < dimen; t0 += (long long)gridDim.x * G3_TR) {
+        const long long r = t0 + lane;
+        const bool in = r < dimen;
+        // digits of the tile's rows (warp 0, a lane per row)
+        if (wid == 0 && in) {
+            long long rem = r;
+            for (int k = 0; k < M; ++k) {
+                const long long sh = ssh[k];
+                const int d = small ? (int)((unsigned)rem / (unsigned)sh) : (int)(rem / sh);
+                rem -= (long long)d * sh;
+                sdig[lane * M + k] = d;
+            }
+        }
+        __syncthreads();
+        // column families: a warp per (state, mode) or (state, pair of modes), a lane per row,
+        // so each gather of a warp reads consecutive rows
+        double *a = sA + lane * nA, *b = sB + lane * nB1;
+        if (wid < S) {
+            const int s = wid;
+            a[s] = in ? (double)u[(long long)s * dimen + r] : 0.0;
+            b[s] = in ? (double)v[(long long)s * dimen + r] : 0.0;
+        }
+#pragma unroll 2
+        for (int f = wid; f < S * M; f += nwarp) {
+            const int s = f / M, k = f - s * M;
+            double xu = 0.0, xv = 0.0, x2u = 0.0, x2v = 0.0, x3v = 0.0, hv = 0.0;
+            if (in) {
+                const T *ur = u + (long long)s * dimen + r, *vr = v + (long long)s * dimen + r;
+                const int d = sdig[lane * M + k], nf = snf[k];
+                const long long sh = ssh[k];
+                const double u0 = (double)ur[0], v0 = (double)vr[0];
+                x2u = D2[d] * u0;
+                x2v = D2[d] * v0;
+                hv = ((double)d + 0.5) * v0;
+                if (d + 1 < nf) {
+                    const double up = (double)ur[sh], vp = (double)vr[sh];
+                    xu += E1[d] * up;
+                    xv += E1[d] * vp;
+                    x3v += E31[d] * vp;
+                }
+                if (d >= 1) {
+                    const double um = (double)ur[-sh], vm = (double)vr[-sh];
+                    xu += E1[d - 1] * um;
+                    xv += E1[d - 1] * vm;
+                    x3v += E31[d - 1] * vm;
+                }
+                if (d + 2 < nf) {
+                    x2u += E2[d] * (double)ur[2 * sh];
+                    x2v += E2[d] * (double)vr[2 * sh];
+                }
+                if (d >= 2) {
+                    x2u += E2[d - 2] * (double)ur[-2 * sh];
+                    x2v += E2[d - 2] * (double)vr[-2 * sh];
+                }
+                if (d + 3 < nf) x3v += E33[d] * (double)vr[3 * sh];
+                if (d >= 3) x3v += E33[d - 3] * (double)vr[-3 * sh];
+            }
+            a[S + k * S + s] = xu;
+            a[S + MS + k * S + s] = x2u;
+            b[S + k * S + s] = xv;
+            b[S + MS + k * S + s] = x2v;
+            b[S + 2 * MS + k * S + s] = hv;
+            b[S + 3 * MS + k * S + s] = x3v;
+        }
+#pragma unroll 2
+        for (int f = wid; f < S * P2; f += nwarp) {
+            const int s = f / P2, p = f - s * P2, l = spair[p] & 255, m = spair[p] >> 8;
+            double xx = 0.0;
+            if (in) {
+                const T *vr = v + (long long)s * dimen + r;
+                const int dl = sdig[lane * M + l], dm = sdig[lane * M + m], nl = snf[l], nm = snf[m];
+                const long long shl = ssh[l], shm = ssh[m];
+                const bool lp = dl + 1 < nl, lm = dl >= 1, mp = dm + 1 < nm, mm = dm >= 1;
+                const double elp = lp ? E1[dl] : 0.0, elm = lm ? E1[dl - 1] : 0.0;
+                const double emp = mp ? E1[dm] : 0.0, emm = mm ? E1[dm - 1] : 0.0;
+                if (lp && mp) xx += elp * emp * (double)vr[shl + shm];
+                if (lp && mm) xx += elp * emm * (double)vr[shl - shm];
+                if (lm && mp) xx += elm * emp * (double)vr[shm - shl];
+                if (lm && mm) xx += elm * emm * (double)vr[-shl - shm];
+            }
+            b[S + 4 * MS + p * S + s] = xx;
+        }
+        __syncthreads();
+        // Gram sums over the tile's rows: 4 outputs per task, no branches
+#pragma unroll
+        for (int j = 0; j < TPT; ++j) {
+            const double *pa = sA + ia[j];
+            const double *p0 = sB + jb[j][0], *p1 = sB + jb[j][1], *p2 = sB + jb[j][2], *p3 = sB + jb[j][3];
+            double c0 = acc[j][0], c1 = acc[j][1], c2 = acc[j][2], c3 = acc[j][3];
+#pragma unroll 8
+            for (int rr = 0; rr < G3_TR; ++rr) {
+                const double av = pa[rr * nA];
+                c0 += av * p0[rr * nB1];
+                c1 += av * p1[rr * nB1];
+                c2 += av * p2[rr * nB1];
+                c3 += av * p3[rr * nB1];
+            }
+            acc[j][0] = c0;
+            acc[j][1] = c1;
+            acc[j][2] = c2;
+            acc[j][3] = c3;
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < TPT; ++j) {
+        const int t = tid + j * nth;
+        if (t >= ntask) continue;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (q < nq[j]) {
+                double *pp = part + (long long)blockIdx.x * nout + 4 * t + q;
+                *pp = accumulate ? *pp + acc[j][q] : acc[j][q];
+            }
+    }
+}
+
+// Column indices of the ordr-3 Gram (host side; the kernel lays them out identically).
+struct G3Cols {
+    int S, M, MS, P2, nA, nB;
+    G3Cols(int S_, int M_) : S(S_), M(M_), MS(M_ * S_), P2(M_ * (M_ - 1) / 2) {
+        nA = S + 2 * MS;
+        nB = S + 4 * MS + P2 * S;
+    }
+    int u(int a) const { return a; }
+    int Xu(int k, int a) const { return S + k * S + a; }
+    int x2u(int k, int a) const { return S + MS + k * S + a; }
+    int v(int b) const { return b; }
+    int Xv(int k, int b) const { return S + k * S + b; }
+    int x2v(int k, int b) const { return S + MS + k * S + b; }
+    int hv(int k, int b) const { return S + 2 * MS + k * S + b; }
+    int x3v(int k, int b) const { return S + 3 * MS + k * S + b; }
+    int pair(int l, int m) const { return l * M - l * (l + 1) / 2 + (m - l - 1); }  // l < m
+    int XXv(int l, int m, int b) const { return S + 4 * MS + pair(l, m) * S + b; }
+};
+
+// The task list (A column, up to 4 B columns) and the output index of every needed (A, B) pair.
+static void gram3_tasks(int S, int M, std::vector<G3Task> &tasks, std::vector<int> &index) {
+    const G3Cols c(S, M);
+    tasks.clear();
+    index.assign((size_t)c.nA * c.nB, -1);
+    // the row's B columns in ascending order, dealt to its K tasks round-robin (task k takes
+    // columns k, k + K, k + 2K, k + 3K): neighbouring threads read neighbouring words of a
+    // shared-memory row (no bank conflicts from a 4-column stride)
+    auto row = [&](int ia, std::vector<int> jbs) {
+        std::sort(jbs.begin(), jbs.end());
+        const int n = (int)jbs.size(), K = (n + 3) / 4, t0 = (int)tasks.size();
+        for (int k = 0; k < K; ++k) {
+            G3Task t{};
+            t.ia = (short)ia;
+            for (int q = 0; q < 4 && k + q * K < n; ++q) {
+                t.jb[q] = (short)jbs[k + q * K];
+                index[(size_t)ia * c.nB + jbs[k + q * K]] = 4 * (t0 + k) + q;
+                t.nq = (short)(q + 1);
+            }
+            tasks.push_back(t);
+        }
+    };
+    for (int a = 0; a < S; ++a) {
+        std::vector<int> j;
+        for (int b = 0; b < S; ++b) j.push_back(c.v(b));
+        for (int k = 0; k < M; ++k)
+            for (int b = 0; b < S; ++b) {
+                j.push_back(c.Xv(k, b));
+                j.push_back(c.x2v(k, b));
+                j.push_back(c.hv(k, b));
+                j.push_back(c.x3v(k, b));
+            }
+        row(c.u(a), j);
+    }
+    for (int k = 0; k < M; ++k)
+        for (int a = 0; a < S; ++a) {
+            std::vector<int> j;
+            for (int l = 0; l < M; ++l)
+                if (l != k)
+                    for (int b = 0; b < S; ++b) j.push_back(c.Xv(l, b));
+            for (int l = k + 1; l < M; ++l)
+                for (int m = l + 1; m < M; ++m)
+                    for (int b = 0; b < S; ++b) j.push_back(c.XXv(l, m, b));
+            row(c.Xu(k, a), j);
+            std::vector<int> j2;
+            for (int l = 0; l < M; ++l)
+                if (l != k)
+                    for (int b = 0; b < S; ++b) j2.push_back(c.Xv(l, b));
+            row(c.x2u(k, a), j2);
+        }
+}
+
+static size_t gram3_smem(int S, int M, int nmax) {
+    const G3Cols c(S, M);
+    return (size_t)(G3_TR * (c.nA + c.nB + 1) + 5 * nmax) * sizeof(double) + (size_t)M * sizeof(long long) +
+           (size_t)(G3_TR * M + c.P2 + M) * sizeof(int);
+}
+
+static bool gram3_fits(int S, int M) {
+    if (M > 255) return false;
+    const G3Cols c(S, M);
+    std::vector<G3Task> t;
+    std::vector<int> idx;
+    if (c.nB > 32767 || c.nA > 32767) return false;
+    gram3_tasks(S, M, t, idx);
+    return gram3_smem(S, M, 64) <= 200 * 1024 && t.size() <= (size_t)4 * G3_THREADS;
+}
+
+static int gram3_len(int S, int M) {
+    std::vector<G3Task> t;
+    std::vector<int> idx;
+    gram3_tasks(S, M, t, idx);
+    return 4 * (int)t.size();
+}
+
+// the task table on the device and the grid, once per handle
+static void gram3_setup(nvb_handle *h) {
+    if (h->d_g3task) return;
+    std::vector<G3Task> t;
+    std::vector<int> idx;
+    gram3_tasks(h->sys.S, h->sys.M, t, idx);
+    CK(cudaMalloc(&h->d_g3task, t.size() * sizeof(G3Task)));
+    CK(cudaMemcpy(h->d_g3task, t.data(), t.size() * sizeof(G3Task), cudaMemcpyHostToDevice));
+    h->g3_ntask = (int)t.size();
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    h->g3_grid = (int)std::min<long long>((h->sys.dimen + G3_TR - 1) / G3_TR, (long long)nsm * 2);
+}
+
+static int gram3_grid(const nvb_handle *h) {
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+    return (int)std::min<long long>((h->sys.dimen + G3_TR - 1) / G3_TR, (long long)nsm * 2);
+}
+
+template <typename T, int TPT>
+static void gram3_kernel(nvb_handle *h, const T *u, const T *v, int accumulate, double *part, size_t shm) {
+    auto k = k_adj_gram3<T, TPT>;
+    if (shm > 48 * 1024) CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    const Plan &pl = h->plan;
+    k<<<h->g3_grid, G3_THREADS, shm, h->stream>>>(u, v, pl.d_etab, pl.nmax, pl.d_nfunc, pl.d_shft, h->sys.M, h->sys.S,
+                                                   h->sys.dimen, (const G3Task *)h->d_g3task, h->g3_ntask,
+                                                   accumulate, part);
+}
+
+// G (+)= the ordr-3 Gram entries of (u, v) through block partials part[g3_grid * gram3_len];
+// G == nullptr: only the partials (accumulate: added to those already there).
+template <typename T>
+static void gram3_launch(nvb_handle *h, const T *u, const T *v, double *G, int accumulate, double *part) {
+    const int S = h->sys.S, M = h->sys.M;
+    if (!gram3_fits(S, M)) fail(NVB_ERR_ARG, "adjoint: too many modes x states for the ordr-3 Gram path");
+    gram3_setup(h);
+    const size_t shm = gram3_smem(S, M, h->plan.nmax);
+    if (shm > 227 * 1024) fail(NVB_ERR_ARG, "adjoint: the ordr-3 Gram tile does not fit in shared memory");
+    const int tpt = (h->g3_ntask + G3_THREADS - 1) / G3_THREADS;
+    const int acc = G ? 0 : accumulate;
+    switch (tpt) {
+    case 1: gram3_kernel<T, 1>(h, u, v, acc, part, shm); break;
+    case 2: gram3_kernel<T, 2>(h, u, v, acc, part, shm); break;
+    case 3: gram3_kernel<T, 3>(h, u, v, acc, part, shm); break;
+    default: gram3_kernel<T, 4>(h, u, v, acc, part, shm); break;
+    }
+    const int nout = 4 * h->g3_ntask;
+    if (G) k_gram_reduce<<<(nout * 32 + 255) / 256, 256, 0, h->stream>>>(part, h->g3_grid, nout, accumulate, G);
+    CK(cudaGetLastError());
+}
+
 static int smax_of(int p, int64_t nf) {
     int s = p;
     while (s > nf - 1) s -= 2;
@@ -429,6 +768,68 @@ static void gram_pc(const nvb_handle *h, const std::vector<double> &Gh, const st
         for (int a = 0; a < S; ++a) Cq[S * S + k] += g(a, S + 2 * M * S + k * S + a);
 }
 
+// P[m][a][b] for the monomials of an ordr-3 system and Cq = (C[a][b], K_k) from the Gram
+// entries (host copy Gh of length gram3_len, laid out by gram3_tasks)
+static void gram3_pc(const nvb_handle *h, const std::vector<double> &Gh, const std::vector<Mono> &monos,
+                     std::vector<double> &P, std::vector<double> &Cq) {
+    const int S = h->sys.S, M = h->sys.M;
+    const G3Cols c(S, M);
+    std::vector<G3Task> tasks;
+    std::vector<int> index;
+    gram3_tasks(S, M, tasks, index);
+    auto G = [&](int ia, int jb) {
+        const int o = index[(size_t)ia * c.nB + jb];
+        if (o < 0) fail(NVB_ERR_STATE, "adjoint: Gram entry not formed");
+        return Gh[(size_t)o];
+    };
+    const int nm = (int)monos.size();
+    P.assign((size_t)nm * S * S, 0.0);
+    for (int t = 0; t < nm; ++t) {
+        const Mono &mo = monos[t];
+        int deg = 0;
+        for (int pw : mo.pows) deg += pw;
+        for (int a = 0; a < S; ++a)
+            for (int b = 0; b < S; ++b) {
+                double val = 0.0;
+                if (mo.modes.size() == 1) {
+                    const int k = mo.modes[0];
+                    if (deg == 1) val = G(c.u(a), c.Xv(k, b));
+                    else if (deg == 2) val = G(c.u(a), c.x2v(k, b));
+                    else val = G(c.u(a), c.x3v(k, b));
+                } else if (mo.modes.size() == 2) {
+                    const int k0 = mo.modes[0], k1 = mo.modes[1];
+                    if (deg == 2) val = G(c.Xu(k0, a), c.Xv(k1, b));
+                    else if (mo.pows[0] == 2) val = G(c.x2u(k0, a), c.Xv(k1, b));  // x_k0^2 x_k1
+                    else val = G(c.x2u(k1, a), c.Xv(k0, b));                      // x_k0 x_k1^2
+                } else {
+                    int k[3] = {mo.modes[0], mo.modes[1], mo.modes[2]};
+                    std::sort(k, k + 3);
+                    val = G(c.Xu(k[0], a), c.XXv(k[1], k[2], b));
+                }
+                P[(size_t)t * S * S + a * S + b] = val;
+            }
+    }
+    Cq.assign((size_t)S * S + M, 0.0);
+    for (int a = 0; a < S; ++a)
+        for (int b = 0; b < S; ++b) Cq[a * S + b] = G(c.u(a), c.v(b));
+    for (int k = 0; k < M; ++k)
+        for (int a = 0; a < S; ++a) Cq[S * S + k] += G(c.u(a), c.hv(k, a));
+}
+
+template <typename T>
+static void gram3_adjoint(nvb_handle *h, const T *u, const T *v, const std::vector<Mono> &monos, std::vector<double> &P,
+                          std::vector<double> &Cq) {
+    gram3_setup(h);
+    const int nout = 4 * h->g3_ntask, grid = h->g3_grid;
+    double *part = (double *)scratch_vector(h, ((size_t)grid + 1) * nout * sizeof(double));
+    double *G = part + (size_t)grid * nout;
+    gram3_launch<T>(h, u, v, G, 0, part);
+    std::vector<double> Gh(nout);
+    CK(cudaMemcpyAsync(Gh.data(), G, nout * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    gram3_pc(h, Gh, monos, P, Cq);
+}
+
 template <typename T>
 static void gram_adjoint(nvb_handle *h, const T *u, const T *v, const std::vector<Mono> &monos, std::vector<double> &P,
                          std::vector<double> &Cq) {
@@ -513,6 +914,8 @@ static void adjoint_s(nvb_handle *h, const T *u, const T *v, double *grad) {
     std::vector<double> Cq;
     if (sys.ordr <= 2 && gram_fits(S, M)) {
         gram_adjoint<T>(h, u, v, monos, P, Cq);
+    } else if (sys.ordr == 3 && gram3_fits(S, M)) {
+        gram3_adjoint<T>(h, u, v, monos, P, Cq);
     } else {
     double *part = nullptr;
     CK(cudaMalloc((void **)&part, (size_t)grid * std::max(TB * S * S, S * S + M) * sizeof(double)));
@@ -595,19 +998,31 @@ void hv_adjoint(nvb_handle *h, const void *u, const void *v, int dtype, double *
 // Accumulated adjoint for the reverse sweep (ordr <= 2 systems whose Gram matrices fit): the
 // gradient is linear in the Gram matrices, so the sweep sums them on the device over all
 // steps and assembles the gradient once.
+static bool gram3_path(const nvb_handle *h) { return h->sys.ordr == 3 && gram3_fits(h->sys.S, h->sys.M); }
+
 int64_t adjoint_gram_len(const nvb_handle *h) {
-    return (h->sys.ordr <= 2 && gram_fits(h->sys.S, h->sys.M)) ? gram_len(h->sys.S, h->sys.M) : 0;
+    if (h->sys.ordr <= 2 && gram_fits(h->sys.S, h->sys.M)) return gram_len(h->sys.S, h->sys.M);
+    if (gram3_path(h)) return gram3_len(h->sys.S, h->sys.M);
+    return 0;
 }
-int64_t adjoint_gram_part_len(const nvb_handle *h) { return (int64_t)gram_grid(h) * adjoint_gram_len(h); }
+int64_t adjoint_gram_part_len(const nvb_handle *h) {
+    return (int64_t)(gram3_path(h) ? gram3_grid(h) : gram_grid(h)) * adjoint_gram_len(h);
+}
 
 void adjoint_gram_add(nvb_handle *h, const void *u, const void *v, int dtype, double *G, int accumulate, double *part) {
+    if (gram3_path(h)) {
+        if (dtype == NVB_DTYPE_F32) gram3_launch<float>(h, (const float *)u, (const float *)v, G, accumulate, part);
+        else gram3_launch<double>(h, (const double *)u, (const double *)v, G, accumulate, part);
+        return;
+    }
     if (dtype == NVB_DTYPE_F32) gram_launch<float>(h, (const float *)u, (const float *)v, G, accumulate, part);
     else gram_launch<double>(h, (const double *)u, (const double *)v, G, accumulate, part);
 }
 
 void adjoint_gram_reduce(nvb_handle *h, const double *part, double *G) {
     const int nout = (int)adjoint_gram_len(h);
-    k_gram_reduce<<<(nout * 32 + 255) / 256, 256, 0, h->stream>>>(part, gram_grid(h), nout, 0, G);
+    const int grid = gram3_path(h) ? gram3_grid(h) : gram_grid(h);
+    k_gram_reduce<<<(nout * 32 + 255) / 256, 256, 0, h->stream>>>(part, grid, nout, 0, G);
     CK(cudaGetLastError());
 }
 
@@ -619,7 +1034,8 @@ void adjoint_gram_grad(nvb_handle *h, const double *G, double *grad) {
     CK(cudaStreamSynchronize(h->stream));
     const auto monos = all_monomials(h->sys);
     std::vector<double> P, Cq;
-    gram_pc(h, Gh, monos, P, Cq);
+    if (gram3_path(h)) gram3_pc(h, Gh, monos, P, Cq);
+    else gram_pc(h, Gh, monos, P, Cq);
     assemble_grad(h, monos, P, Cq, grad);
 }
 

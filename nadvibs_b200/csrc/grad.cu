@@ -56,6 +56,22 @@ int grid_g(long long n) {
     return (int)std::max<long long>(b, 1);
 }
 
+__global__ void k_to_f32(float *__restrict__ dst, const double *__restrict__ src, long long n) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = (float)src[i];
+}
+
+// A mixed-precision handle whose FP64 products have no factorised kernel (a pencil too wide for
+// the FP64 register state) while its FP32 products have one: the reverse sweep forms H wbar in
+// FP32 through the factorised kernel (the forward's own precision; ~1e-7 relative per product)
+// instead of the general FP64 kernel, at the cost of two FP32 work vectors.
+static bool sweep_hv_f32(const nvb_handle *h) {
+    if (h->precision != NVB_MIXED) return false;
+    const bool f64 = h->quad.ok || (h->cubic.ok && h->cubic.prec_ok[0]);
+    const bool f32 = h->quad.ok || (h->cubic.ok && h->cubic.prec_ok[1]);
+    return !f64 && f32;
+}
+
 template <typename T>
 __global__ void k_to_f64(double *__restrict__ dst, const T *__restrict__ src, double sc, long long n) {
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -160,7 +176,8 @@ static void rec_reserve(nvb_handle *h, int64_t total_iters) {
     CK(cudaMemGetInfo(&freeb, &totalb));
     const double held = h->rec_ok ? (double)(2 * h->rec_cap + 2) * (double)per : 0.0;
     const double budget = h->grad_budget > 0 ? (double)h->grad_budget : 0.85 * ((double)freeb + held);
-    const double need = (double)(2 * total_iters + 2) * (double)per + 5.0 * (double)per + 10.0 * (double)per64;
+    const double need = (double)(2 * total_iters + 2) * (double)per + (sweep_hv_f32(h) ? 7.0 : 5.0) * (double)per +
+                        10.0 * (double)per64;
     if (need > budget) {
         rec_free(h);
         return;
@@ -346,6 +363,7 @@ struct Sweep {
     std::vector<double> segs;                // their scales
     double *vb_next = nullptr, *vb_cur = nullptr, *vb_prev = nullptr, *rbar = nullptr, *wbar = nullptr,
            *wv = nullptr, *v64[3] = {nullptr, nullptr, nullptr}, *w64 = nullptr;
+    float *w32a = nullptr, *w32b = nullptr;  // H wbar in FP32 (sweep_hv_f32)
     std::vector<double> abar, bbar, gstep;
     double *grad = nullptr;
     int64_t nc = 0, replayed = 0;  // H.v applications of the replays
@@ -432,7 +450,13 @@ struct Sweep {
             }
             k_step<<<g, 256, 0, h->stream>>>(vb_cur, wbar, vb_prev, rbar, wi, vi, al, abar[i - 1], d_dots + 1, bprev,
                                              i > 1 ? 1 : 0, N);
-            hv_any(h, wbar, wv, NVB_DTYPE_F64, nullptr, nullptr, nullptr);  // H wbar
+            if (w32a) {  // H wbar through the FP32 factorised kernel
+                k_to_f32<<<g, 256, 0, h->stream>>>(w32a, wbar, N);
+                hv_any(h, w32a, w32b, NVB_DTYPE_F32, nullptr, nullptr, nullptr);
+                k_to_f64<float><<<g, 256, 0, h->stream>>>(wv, w32b, 1.0, N);
+            } else {
+                hv_any(h, wbar, wv, NVB_DTYPE_F64, nullptr, nullptr, nullptr);  // H wbar
+            }
             k_lin<<<g, 256, 0, h->stream>>>(vb_cur, 1.0, wv, 0.0, nullptr, 1, N);
             CK(cudaGetLastError());
             if (G) {
@@ -569,7 +593,7 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
         size_t freeb = 0, totalb = 0;
         CK(cudaMemGetInfo(&freeb, &totalb));
         const double budget = h->grad_budget > 0 ? (double)h->grad_budget : 0.85 * (double)freeb;
-        const double fixed = 5.0 * (double)W.per + 10.0 * (double)W.per64;
+        const double fixed = (sweep_hv_f32(h) ? 7.0 : 5.0) * (double)W.per + 10.0 * (double)W.per64;
         int64_t L = 0;
         if (!plan_levels(span, (budget - fixed) / (double)W.per, &L, &W.B, &W.bmax))
             fail(NVB_ERR_NOMEM, "the reverse sweep does not fit the device-memory budget");
@@ -584,6 +608,10 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
         b0(nbase * W.per), b1(nbase * W.per), b2(nbase * W.per);
     DevBuf vbn(W.per64), vbc(W.per64), vbp(W.per64), rb(W.per64), wb(W.per64), wvb(W.per64), c0(W.per64),
         c1(W.per64), c2(W.per64), cw(W.per64);
+    const bool h32 = sweep_hv_f32(h);
+    DevBuf w32a(h32 ? W.per : 0), w32b(h32 ? W.per : 0);
+    W.w32a = (float *)w32a.p;
+    W.w32b = (float *)w32b.p;
     W.segv = segv.p;
     W.segw = segw.p;
     W.segs.assign(W.bmax + 2, 0.0);

@@ -38,10 +38,16 @@ def _unflatten(pot_flat, nb, ordr, M):
     return out
 
 
-@pytest.mark.parametrize("seed,nstates,basis,ordr", [(41, 2, [4, 3, 3], 2), (42, 3, [3, 3, 2], 3),
-                                                     (43, 1, [5, 4], 4), (44, 2, [4, 4, 3], 2)])
+# ordr 3 runs the cubic Gram path (every P_m an entry of (X u, x^2 u)^T (v, X v, x^2 v, x^3 v,
+# X X v)): cases with several distinct triples of modes, 1- and 2-function modes, up to 4 states
+# and both settings of the x^3 quirk
+@pytest.mark.parametrize("seed,nstates,basis,ordr,qc", [(41, 2, [4, 3, 3], 2, 1), (42, 3, [3, 3, 2], 3, 1),
+                                                        (43, 1, [5, 4], 4, 1), (44, 2, [4, 4, 3], 2, 1),
+                                                        (45, 2, [4, 3, 2, 3], 3, 1), (45, 2, [4, 3, 2, 3], 3, 0),
+                                                        (46, 1, [5, 3, 4, 2, 3], 3, 1), (47, 4, [2, 3, 2, 2], 3, 0),
+                                                        (48, 2, [3, 1, 4, 3], 3, 1)])
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
-def test_adjoint_matches_finite_differences(seed, nstates, basis, ordr, dt):
+def test_adjoint_matches_finite_differences(seed, nstates, basis, ordr, qc, dt):
     cfg = synth.random_small(seed, nstates, basis, ordr)
     om, cc, pot = synth.draw_small(cfg)
     M = len(basis)
@@ -49,11 +55,11 @@ def test_adjoint_matches_finite_differences(seed, nstates, basis, ordr, dt):
     potf = synth.flatten_pot(pot)
     npot = len(potf)
     theta = np.concatenate([potf, cc, om])
-    S = O.system_from_arrays(basis, nstates, ordr, om, cc, pot, quirk_lower=False)
+    S = O.system_from_arrays(basis, nstates, ordr, om, cc, pot, quirk_lower=False, quirk_cubic=bool(qc))
     rng = np.random.default_rng(seed)
     u = rng.normal(size=S.ntotal)
     v = rng.normal(size=S.ntotal)
-    with L.Handle.from_arrays(_params(nstates, basis, ordr), om, cc, potf, quirk_lower=0) as h:
+    with L.Handle.from_arrays(_params(nstates, basis, ordr), om, cc, potf, quirk_lower=0, quirk_cubic=qc) as h:
         ut = torch.from_numpy(u).to("cuda", dtype=dt)
         vt = torch.from_numpy(v).to("cuda", dtype=dt)
         torch.cuda.synchronize()
@@ -65,7 +71,7 @@ def test_adjoint_matches_finite_differences(seed, nstates, basis, ordr, dt):
     def f(th):
         w, c, p = _split(th, npot, nb, M)
         Sx = O.system_from_arrays(basis, nstates, ordr, w, c, _unflatten(p, nb, ordr, M), quirk_lower=False,
-                                  ztoler=0.0)
+                                  quirk_cubic=bool(qc), ztoler=0.0)
         return float(u @ Sx.hv(v))
 
     fd = np.zeros_like(theta)
