@@ -341,7 +341,7 @@ __global__ void k_gram_reduce(const double *__restrict__ part, int ng, int nout,
 // reads consecutive rows), then every thread accumulates its tasks over the tile's rows.
 // Block partials are summed in a fixed order.
 
-constexpr int G3_TR = 32;
+constexpr int G3_TR = 64;  // rows per tile: two per lane
 constexpr int G3_THREADS = 512;
 struct G3Task {
     short ia, nq;
@@ -401,37 +401,46 @@ __global__ void __launch_bounds__(G3_THREADS, 1) k_adj_gram3(const T *__restrict
         }
     }
     __syncthreads();
-    static_assert(G3_TR == 32, "one lane per row of the tile");
+    static_assert(G3_TR % 32 == 0, "whole warps of rows");
     const int lane = tid & 31, wid = tid >> 5, nwarp = nth >> 5;
     for (long long t0 = (long long)blockIdx.x * G3_TR; t0 < dimen; t0 += (long long)gridDim.x * G3_TR) {
-        const long long r = t0 + lane;
-        const bool in = r < dimen;
-        // digits of the tile's rows (warp 0, a lane per row)
-        if (wid == 0 && in) {
+        // digits of the tile's rows (one thread per row)
+        for (int e = tid; e < G3_TR; e += nth) {
+            const long long r = t0 + e;
+            if (r >= dimen) continue;
             long long rem = r;
             for (int k = 0; k < M; ++k) {
                 const long long sh = ssh[k];
                 const int d = small ? (int)((unsigned)rem / (unsigned)sh) : (int)(rem / sh);
                 rem -= (long long)d * sh;
-                sdig[lane * M + k] = d;
+                sdig[e * M + k] = d;
             }
         }
         __syncthreads();
-        // column families: a warp per (state, mode) or (state, pair of modes), a lane per row,
-        // so each gather of a warp reads consecutive rows
-        double *a = sA + lane * nA, *b = sB + lane * nB1;
+        // column families: a warp per (state, mode) or (state, pair of modes), a lane per row
+        // (G3_TR / 32 rows per lane), so each gather of a warp reads consecutive rows
         if (wid < S) {
             const int s = wid;
-            a[s] = in ? (double)u[(long long)s * dimen + r] : 0.0;
-            b[s] = in ? (double)v[(long long)s * dimen + r] : 0.0;
+#pragma unroll
+            for (int hr = 0; hr < G3_TR / 32; ++hr) {
+                const int e = lane + 32 * hr;
+                const long long r = t0 + e;
+                sA[e * nA + s] = r < dimen ? (double)u[(long long)s * dimen + r] : 0.0;
+                sB[e * nB1 + s] = r < dimen ? (double)v[(long long)s * dimen + r] : 0.0;
+            }
         }
-#pragma unroll 2
-        for (int f = wid; f < S * M; f += nwarp) {
+        for (int f = wid; f < S * M; f += nwarp)
+#pragma unroll
+        for (int hr = 0; hr < G3_TR / 32; ++hr) {
+            const int e = lane + 32 * hr;
+            const long long r = t0 + e;
+            const bool in = r < dimen;
+            double *a = sA + e * nA, *b = sB + e * nB1;
             const int s = f / M, k = f - s * M;
             double xu = 0.0, xv = 0.0, x2u = 0.0, x2v = 0.0, x3v = 0.0, hv = 0.0;
             if (in) {
                 const T *ur = u + (long long)s * dimen + r, *vr = v + (long long)s * dimen + r;
-                const int d = sdig[lane * M + k], nf = snf[k];
+                const int d = sdig[e * M + k], nf = snf[k];
                 const long long sh = ssh[k];
                 const double u0 = (double)ur[0], v0 = (double)vr[0];
                 x2u = D2[d] * u0;
@@ -467,13 +476,18 @@ __global__ void __launch_bounds__(G3_THREADS, 1) k_adj_gram3(const T *__restrict
             b[S + 2 * MS + k * S + s] = hv;
             b[S + 3 * MS + k * S + s] = x3v;
         }
-#pragma unroll 2
-        for (int f = wid; f < S * P2; f += nwarp) {
+        for (int f = wid; f < S * P2; f += nwarp)
+#pragma unroll
+        for (int hr = 0; hr < G3_TR / 32; ++hr) {
+            const int e = lane + 32 * hr;
+            const long long r = t0 + e;
+            const bool in = r < dimen;
+            double *b = sB + e * nB1;
             const int s = f / P2, p = f - s * P2, l = spair[p] & 255, m = spair[p] >> 8;
             double xx = 0.0;
             if (in) {
                 const T *vr = v + (long long)s * dimen + r;
-                const int dl = sdig[lane * M + l], dm = sdig[lane * M + m], nl = snf[l], nm = snf[m];
+                const int dl = sdig[e * M + l], dm = sdig[e * M + m], nl = snf[l], nm = snf[m];
                 const long long shl = ssh[l], shm = ssh[m];
                 const bool lp = dl + 1 < nl, lm = dl >= 1, mp = dm + 1 < nm, mm = dm >= 1;
                 const double elp = lp ? E1[dl] : 0.0, elm = lm ? E1[dl - 1] : 0.0;
