@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both")
     ap.add_argument("--hv-only", action="store_true", help="run H.v launches only (profiling)")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run the adjoint contraction d<u|H|v>/dtheta only (FP64 vectors; profiling)")
     ap.add_argument("--grad-only", action="store_true",
                     help="run the gradient leg only and print its JSON (profiling)")
     ap.add_argument("--config", type=int, default=CONFIG_NUMBER)
@@ -389,6 +391,41 @@ def grad_timing(dev: int):
             "grad_over_fwd": g / f}
 
 
+def adjoint_timing(args, dev: int) -> dict:
+    """warmup + steps calls of the adjoint contraction (nvb_hv_adjoint_coeffs) of the chosen
+    system with random FP64 u, v; host wall time per call around synchronised calls."""
+    import numpy as np
+    import torch
+    from nadvibs_b200 import _lib as L
+    from nadvibs_b200 import synth
+    torch.cuda.set_device(dev)
+    cfg = synth.config(args.config)
+    if args.basis:
+        cfg.basis = [int(b) for b in args.basis.split(",")]
+    om, cc, pot = synth.draw(cfg)
+    p = L.default_params()
+    p.nstates, p.nmodes, p.ordr, p.niter = cfg.nstates, cfg.nmodes, cfg.ordr, 10
+    for i, b in enumerate(cfg.basis):
+        p.basis[i] = b
+    n = int(np.prod(cfg.basis)) * cfg.nstates
+    h = L.Handle.from_arrays(p, om, cc, synth.flatten_pot(pot), device=dev, precision=L.NVB_MIXED, quirk_lower=0)
+    try:
+        g = torch.Generator(device=f"cuda:{dev}").manual_seed(1)
+        u = torch.randn(n, generator=g, device=f"cuda:{dev}", dtype=torch.float64)
+        v = torch.randn(n, generator=g, device=f"cuda:{dev}", dtype=torch.float64)
+        for _ in range(args.warmup):
+            h.adjoint_ptr(u.data_ptr(), v.data_ptr(), L.DTYPE_F64)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            h.adjoint_ptr(u.data_ptr(), v.data_ptr(), L.DTYPE_F64)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3 / max(args.steps, 1)
+    finally:
+        h.close()
+    return {"basis": list(cfg.basis), "elements": n, "ms_per_call": ms}
+
+
 def tile_stream(stream: dict | None, hv_ms: float, seconds: float = 1.0):
     """The factorised H.v's neighbour-tile stream (bytes copied L2 -> shared memory per product)
     against its measured ceiling: whole tiles of the same size streamed into a ring of the same
@@ -566,6 +603,10 @@ def main():
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "iter/s", "h2d_bytes_per_step": 0,
                                             "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
+        return 0
+    if args.adjoint_only:
+        if rank == 0:
+            print(json.dumps({"adjoint_only": adjoint_timing(args, local)}))
         return 0
     if args.grad_only:
         if rank == 0:
