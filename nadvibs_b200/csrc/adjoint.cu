@@ -335,38 +335,60 @@ __global__ void k_gram_reduce(const double *__restrict__ part, int ng, int nout,
 //   x_k: <u_a, X_k v_b>   x_k^2: <u_a, x_k^2 v_b>   x_k^3: <u_a, x_k^3 v_b>
 //   x_k x_l: <X_k u_a, X_l v_b>   x_k^2 x_l: <x_k^2 u_a, X_l v_b>
 //   x_k x_l x_m (k < l < m): <X_k u_a, X_l X_m v_b>,   C = <u_a, v_b>,   K_k = sum_a <u_a, (n_k+1/2) v_a>.
-// Only those entries are formed: a task list of (A column, up to 4 B columns).  Per tile of
-// G3_TR = 32 rows the columns are expanded into shared memory (digits decoded once per row;
-// a warp per (state, mode) or (state, pair of modes) family and a lane per row, so each gather
-// reads consecutive rows), then every thread accumulates its tasks over the tile's rows.
-// Block partials are summed in a fixed order.
+// The sums over rows run on the FP64 tensor cores (mma m8n8k4): G is cut into 8 x 8 blocks
+// (8 A columns x 8 B columns) and only the blocks holding a needed entry are formed.  The B
+// columns are ordered so that the needed entries cluster: X v first, then v, x^2 v,
+// (n+1/2) v, x^3 v, then X_l X_m v by descending l (an A column X_k u needs exactly the pairs
+// with l > k, a prefix).  Per tile of TR rows the columns are expanded into shared memory
+// (column-major, a warp per mode or pair of modes over all states, a lane per row, element
+// tables in shared memory), then each warp runs its blocks' MMAs over the tile.  Block partials
+// are summed in a fixed order.
 
-constexpr int G3_TR = 64;  // rows per tile: two per lane
 constexpr int G3_THREADS = 512;
-struct G3Task {
-    short ia, nq;
-    short jb[4];
+constexpr int G3_NBW = 8;  // most MMA blocks per warp
+constexpr int G3_SMAX = 4; // most electronic states
+
+// Shared-memory column positions of the ordr-3 Gram columns (A as logical; B regrouped).
+struct G3Pos {
+    int nA8, XO, PO, nB8;
+    __host__ __device__ G3Pos(int S, int M) {
+        const int MS = M * S, P2 = M * (M - 1) / 2;
+        nA8 = (S + 2 * MS + 7) & ~7;
+        XO = (MS + 7) & ~7;                   // v, x^2 v, (n+1/2) v, x^3 v
+        PO = (XO + S + 3 * MS + 7) & ~7;      // X_l X_m v
+        nB8 = (PO + P2 * S + 7) & ~7;
+    }
 };
 
-template <typename T, int TPT>
-__global__ void __launch_bounds__(G3_THREADS, 1) k_adj_gram3(const T *__restrict__ u, const T *__restrict__ v,
-                                                          const double *__restrict__ etab, int nmax,
-                                                          const int *__restrict__ nfunc,
-                                                          const long long *__restrict__ shft, int M, int S,
-                                                          long long dimen, const G3Task *__restrict__ tasks,
-                                                          int ntask, int accumulate, double *__restrict__ part) {
+__device__ __forceinline__ void mma_f64_884(double (&c)[2], double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(c[0]), "+d"(c[1])
+        : "d"(a), "d"(b));
+}
+
+// TR rows per tile (a multiple of 32); column pitch TR + 4 doubles, so the 4 x 4 fragment of
+// each half-warp (4 rows of 4 columns) covers all 32 banks; NBW: most MMA blocks per warp.
+// NBUF = 2: two column tiles, so one barrier per tile separates the expansion of tile i (and the
+// digits of tile i+1) from the MMAs of tile i-1, and warps in either phase overlap; NBUF = 1:
+// one tile, expansion and MMAs separated by barriers.
+template <typename T, int TR, int NBW, int NBUF>
+__global__ void __launch_bounds__(G3_THREADS, 1)
+    k_adj_gram3(const T *__restrict__ u, const T *__restrict__ v, const double *__restrict__ etab, int nmax,
+                const int *__restrict__ nfunc, const long long *__restrict__ shft, int M, int S, long long dimen,
+                const int *__restrict__ blocks, int nblk, int nbw, int accumulate, double *__restrict__ part) {
+    constexpr int PT = TR + 4, RPL = TR / 32;
+    static_assert(TR % 32 == 0, "whole warps of rows");
     extern __shared__ double sm[];
-    const int MS = M * S, P2 = M * (M - 1) / 2, nA = S + 2 * MS, nB = S + 4 * MS + P2 * S;
-    const int nB1 = nB + 1;  // column nB stays zero: the padding of tasks with fewer than 4 outputs
-    const int nout = 4 * ntask;
-    double *sA = sm, *sB = sm + G3_TR * nA;             // [row][col]
-    double *stab = sB + G3_TR * nB1;                     // element rows E1, E2, D2, E31, E33 [nmax]
-    long long *ssh = reinterpret_cast<long long *>(stab + 5 * nmax);  // [M] strides
-    int *sdig = reinterpret_cast<int *>(ssh + M);        // [row][mode]
-    int *spair = sdig + G3_TR * M;                       // pair p: l | m << 8
-    int *snf = spair + P2;                               // [M] nfunc
-    const int tid = threadIdx.x, nth = blockDim.x;
-    const bool small = dimen <= 0xFFFFFFFFll;
+    const int MS = M * S, P2 = M * (M - 1) / 2;
+    const G3Pos ps(S, M);
+    const int tcols = (ps.nA8 + ps.nB8) * PT;                  // one column tile: A then B, [column][row]
+    double *stab = sm + NBUF * tcols;                          // element rows E1, E2, D2, E31, E33 [nmax]
+    int *ssh = reinterpret_cast<int *>(stab + 5 * nmax);       // [M] strides
+    int *snf = ssh + M;                                        // [M] nfunc
+    int *spair = snf + M;                                      // pair p (descending l): l | m << 8
+    int *sdig0 = spair + P2;                                   // [NBUF][mode][row]
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, wid = tid >> 5, nwarp = nth >> 5;
+    for (int i = tid; i < NBUF * tcols; i += nth) sm[i] = 0.0;  // padding columns stay zero
     for (int i = tid; i < nmax; i += nth) {
         stab[0 * nmax + i] = etab[(0 * ETAB_J + 1) * nmax + i];  // <n|x|n+1>
         stab[1 * nmax + i] = etab[(1 * ETAB_J + 2) * nmax + i];  // <n|x^2|n+2>
@@ -375,166 +397,277 @@ __global__ void __launch_bounds__(G3_THREADS, 1) k_adj_gram3(const T *__restrict
         stab[4 * nmax + i] = etab[(2 * ETAB_J + 3) * nmax + i];  // <n|x^3|n+3>
     }
     for (int k = tid; k < M; k += nth) {
-        ssh[k] = shft[k];
+        ssh[k] = (int)shft[k];
         snf[k] = nfunc[k];
     }
-    for (int e = tid; e < G3_TR; e += nth) sB[e * nB1 + nB] = 0.0;
     if (tid == 0) {
         int q = 0;
-        for (int l = 0; l < M; ++l)
+        for (int l = M - 2; l >= 0; --l)
             for (int m = l + 1; m < M; ++m) spair[q++] = l | (m << 8);
     }
     const double *E1 = stab, *E2 = stab + nmax, *D2 = stab + 2 * nmax, *E31 = stab + 3 * nmax, *E33 = stab + 4 * nmax;
-    // this thread's tasks: A column and 4 B columns (padded with the zero column)
-    int ia[TPT], jb[TPT][4], nq[TPT];
-    double acc[TPT][4];
+    // this warp's blocks [wid * nbw, +nq) (nbw <= NBW): fragment offsets of A (column ib*8 + lane/4)
+    // and B (column jb*8 + lane/4) within a column tile, row lane%4 of each 4-row step
+    const int nq = max(0, min(nbw, nblk - wid * nbw));
+    int aoff[NBW], boff[NBW];
+    double acc[NBW][2];
 #pragma unroll
-    for (int j = 0; j < TPT; ++j) {
-        const int t = tid + j * nth;
-        G3Task tk = t < ntask ? tasks[t] : G3Task{0, 0, {0, 0, 0, 0}};
-        ia[j] = tk.ia;
-        nq[j] = tk.nq;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            jb[j][q] = q < tk.nq ? tk.jb[q] : nB;
-            acc[j][q] = 0.0;
-        }
+    for (int q = 0; q < NBW; ++q) {
+        const int w = q < nq ? blocks[wid * nbw + q] : 0;
+        aoff[q] = ((w & 0xffff) * 8 + (lane >> 2)) * PT + (lane & 3);
+        boff[q] = (ps.nA8 + (w >> 16) * 8 + (lane >> 2)) * PT + (lane & 3);
+        acc[q][0] = acc[q][1] = 0.0;
     }
-    __syncthreads();
-    static_assert(G3_TR % 32 == 0, "whole warps of rows");
-    const int lane = tid & 31, wid = tid >> 5, nwarp = nth >> 5;
-    for (long long t0 = (long long)blockIdx.x * G3_TR; t0 < dimen; t0 += (long long)gridDim.x * G3_TR) {
-        // digits of the tile's rows (one thread per row)
-        for (int e = tid; e < G3_TR; e += nth) {
+    const long long tstride = (long long)gridDim.x * TR, first = (long long)blockIdx.x * TR;
+    const int ntl = first < dimen ? (int)((dimen - first + tstride - 1) / tstride) : 0;  // this block's tiles
+    // digits of tile t's rows: a thread per (mode, row)
+    auto digits = [&](int t, int *sdig) {
+        const long long t0 = first + (long long)t * tstride;
+        for (int i = tid; i < M * TR; i += nth) {
+            const int k = i / TR, e = i - k * TR;
             const long long r = t0 + e;
-            if (r >= dimen) continue;
-            long long rem = r;
-            for (int k = 0; k < M; ++k) {
-                const long long sh = ssh[k];
-                const int d = small ? (int)((unsigned)rem / (unsigned)sh) : (int)(rem / sh);
-                rem -= (long long)d * sh;
-                sdig[e * M + k] = d;
+            sdig[i] = r < dimen ? (int)((unsigned)r / (unsigned)ssh[k] % (unsigned)snf[k]) : 0;
+        }
+    };
+    // columns of tile t: families f < MS the (mode, state) pairs, then the pairs of modes over
+    // all states (each about twelve gathers per row), a lane per row
+    auto expand = [&](int t, const int *sdig, double *sA) {
+        double *sB = sA + ps.nA8 * PT;
+        const long long t0 = first + (long long)t * tstride;
+        for (int f = wid; f < MS + P2; f += nwarp) {
+            if (f < MS) {
+                const int k = f / S, s = f - k * S, nf = snf[k], sh = ssh[k];
+#pragma unroll
+                for (int hr = 0; hr < RPL; ++hr) {
+                    const int e = lane + 32 * hr;
+                    const long long r = t0 + e;
+                    const bool in = r < dimen;
+                    const int d = sdig[k * TR + e];
+                    const bool p1 = in && d + 1 < nf, m1 = in && d >= 1, p2 = in && d + 2 < nf, m2 = in && d >= 2;
+                    const bool p3 = in && d + 3 < nf, m3 = in && d >= 3;
+                    const T *ur = u + (long long)s * dimen + (in ? r : 0), *vr = v + (long long)s * dimen + (in ? r : 0);
+                    const double u0 = in ? (double)ur[0] : 0.0, v0 = in ? (double)vr[0] : 0.0;
+                    const double ed2 = in ? D2[d] : 0.0;
+                    double xu = 0.0, xv = 0.0, x2u = ed2 * u0, x2v = ed2 * v0, x3v = 0.0;
+                    if (p1) {
+                        const double up = (double)ur[sh], vp = (double)vr[sh];
+                        xu += E1[d] * up;
+                        xv += E1[d] * vp;
+                        x3v += E31[d] * vp;
+                    }
+                    if (m1) {
+                        const double um = (double)ur[-sh], vm = (double)vr[-sh];
+                        xu += E1[d - 1] * um;
+                        xv += E1[d - 1] * vm;
+                        x3v += E31[d - 1] * vm;
+                    }
+                    if (p2) {
+                        x2u += E2[d] * (double)ur[2 * sh];
+                        x2v += E2[d] * (double)vr[2 * sh];
+                    }
+                    if (m2) {
+                        x2u += E2[d - 2] * (double)ur[-2 * sh];
+                        x2v += E2[d - 2] * (double)vr[-2 * sh];
+                    }
+                    if (p3) x3v += E33[d] * (double)vr[3 * sh];
+                    if (m3) x3v += E33[d - 3] * (double)vr[-3 * sh];
+                    const int c = k * S + s;
+                    if (k == 0) {
+                        sA[s * PT + e] = u0;
+                        sB[(ps.XO + s) * PT + e] = v0;
+                    }
+                    sA[(S + c) * PT + e] = xu;
+                    sA[(S + MS + c) * PT + e] = x2u;
+                    sB[c * PT + e] = xv;
+                    sB[(ps.XO + S + c) * PT + e] = x2v;
+                    sB[(ps.XO + S + MS + c) * PT + e] = ((double)d + 0.5) * v0;
+                    sB[(ps.XO + S + 2 * MS + c) * PT + e] = x3v;
+                }
+            } else {
+                const int pd = f - MS, pw = spair[pd], l = pw & 255, m = pw >> 8;
+                const int nl = snf[l], nm = snf[m], shl = ssh[l], shm = ssh[m];
+#pragma unroll
+                for (int hr = 0; hr < RPL; ++hr) {
+                    const int e = lane + 32 * hr;
+                    const long long r = t0 + e;
+                    const bool in = r < dimen;
+                    const int dl = sdig[l * TR + e], dm = sdig[m * TR + e];
+                    const bool lp = in && dl + 1 < nl, lm = in && dl >= 1, mp = dm + 1 < nm, mm = dm >= 1;
+                    const double elp = lp ? E1[dl] : 0.0, elm = lm ? E1[dl - 1] : 0.0;
+                    const double emp = mp ? E1[dm] : 0.0, emm = mm ? E1[dm - 1] : 0.0;
+                    const bool bpp = lp && mp, bpm = lp && mm, bmp = lm && mp, bmm = lm && mm;
+                    const double cpp = elp * emp, cpm = elp * emm, cmp = elm * emp, cmm = elm * emm;
+                    for (int s = 0; s < S; ++s) {
+                        const T *vr = v + (long long)s * dimen + (in ? r : 0);
+                        double xx = 0.0;
+                        if (bpp) xx += cpp * (double)vr[shl + shm];
+                        if (bpm) xx += cpm * (double)vr[shl - shm];
+                        if (bmp) xx += cmp * (double)vr[shm - shl];
+                        if (bmm) xx += cmm * (double)vr[-shl - shm];
+                        sB[(ps.PO + pd * S + s) * PT + e] = xx;
+                    }
+                }
             }
         }
-        __syncthreads();
-        // column families: a warp per (state, mode) or (state, pair of modes), a lane per row
-        // (G3_TR / 32 rows per lane), so each gather of a warp reads consecutive rows
-        if (wid < S) {
-            const int s = wid;
+    };
+    // The same columns one family at a time with a hook between the gathers and their use:
+    // `between()` runs while the family's loads are in flight (the double-buffered schedule puts
+    // a slice of the previous tile's MMAs there).  Offsets of neighbours outside the basis are
+    // clamped to the row itself and their coefficients are zero, so the loads are unconditional.
+    auto family = [&](int f, int t, const int *sdig, double *sA, auto &&between) {
+        double *sB = sA + ps.nA8 * PT;
+        const long long t0 = first + (long long)t * tstride;  // < dimen: the tile exists
+        if (f < MS) {
+            const int k = f / S, s = f - k * S, nf = snf[k], sh = ssh[k];
+            double g[RPL][12];
 #pragma unroll
-            for (int hr = 0; hr < G3_TR / 32; ++hr) {
+            for (int hr = 0; hr < RPL; ++hr) {
                 const int e = lane + 32 * hr;
                 const long long r = t0 + e;
-                sA[e * nA + s] = r < dimen ? (double)u[(long long)s * dimen + r] : 0.0;
-                sB[e * nB1 + s] = r < dimen ? (double)v[(long long)s * dimen + r] : 0.0;
+                const bool in = r < dimen;
+                const int d = sdig[k * TR + e];
+                const int o1p = in && d + 1 < nf ? sh : 0, o1m = in && d >= 1 ? -sh : 0;
+                const int o2p = in && d + 2 < nf ? 2 * sh : 0, o2m = in && d >= 2 ? -2 * sh : 0;
+                const int o3p = in && d + 3 < nf ? 3 * sh : 0, o3m = in && d >= 3 ? -3 * sh : 0;
+                const long long rr = in ? r : t0;
+                const T *ur = u + (long long)s * dimen + rr, *vr = v + (long long)s * dimen + rr;
+                g[hr][0] = (double)ur[0];
+                g[hr][1] = (double)vr[0];
+                g[hr][2] = (double)ur[o1p];
+                g[hr][3] = (double)vr[o1p];
+                g[hr][4] = (double)ur[o1m];
+                g[hr][5] = (double)vr[o1m];
+                g[hr][6] = (double)ur[o2p];
+                g[hr][7] = (double)vr[o2p];
+                g[hr][8] = (double)ur[o2m];
+                g[hr][9] = (double)vr[o2m];
+                g[hr][10] = (double)vr[o3p];
+                g[hr][11] = (double)vr[o3m];
             }
-        }
-        for (int f = wid; f < S * M; f += nwarp)
+            between();
 #pragma unroll
-        for (int hr = 0; hr < G3_TR / 32; ++hr) {
-            const int e = lane + 32 * hr;
-            const long long r = t0 + e;
-            const bool in = r < dimen;
-            double *a = sA + e * nA, *b = sB + e * nB1;
-            const int s = f / M, k = f - s * M;
-            double xu = 0.0, xv = 0.0, x2u = 0.0, x2v = 0.0, x3v = 0.0, hv = 0.0;
-            if (in) {
-                const T *ur = u + (long long)s * dimen + r, *vr = v + (long long)s * dimen + r;
-                const int d = sdig[e * M + k], nf = snf[k];
-                const long long sh = ssh[k];
-                const double u0 = (double)ur[0], v0 = (double)vr[0];
-                x2u = D2[d] * u0;
-                x2v = D2[d] * v0;
-                hv = ((double)d + 0.5) * v0;
-                if (d + 1 < nf) {
-                    const double up = (double)ur[sh], vp = (double)vr[sh];
-                    xu += E1[d] * up;
-                    xv += E1[d] * vp;
-                    x3v += E31[d] * vp;
+            for (int hr = 0; hr < RPL; ++hr) {
+                const int e = lane + 32 * hr;
+                const bool in = t0 + e < dimen;
+                const int d = sdig[k * TR + e];
+                const bool p1 = in && d + 1 < nf, m1 = in && d >= 1, p2 = in && d + 2 < nf, m2 = in && d >= 2;
+                const bool p3 = in && d + 3 < nf, m3 = in && d >= 3;
+                const double u0 = in ? g[hr][0] : 0.0, v0 = in ? g[hr][1] : 0.0;
+                const double e1p = p1 ? E1[d] : 0.0, e1m = m1 ? E1[d - 1] : 0.0;
+                const double e31p = p1 ? E31[d] : 0.0, e31m = m1 ? E31[d - 1] : 0.0;
+                const double e2p = p2 ? E2[d] : 0.0, e2m = m2 ? E2[d - 2] : 0.0, ed2 = in ? D2[d] : 0.0;
+                const double e33p = p3 ? E33[d] : 0.0, e33m = m3 ? E33[d - 3] : 0.0;
+                const double xu = e1p * g[hr][2] + e1m * g[hr][4];
+                const double xv = e1p * g[hr][3] + e1m * g[hr][5];
+                const double x2u = ed2 * u0 + e2p * g[hr][6] + e2m * g[hr][8];
+                const double x2v = ed2 * v0 + e2p * g[hr][7] + e2m * g[hr][9];
+                const double x3v = e31p * g[hr][3] + e31m * g[hr][5] + e33p * g[hr][10] + e33m * g[hr][11];
+                const int c = k * S + s;
+                if (k == 0) {
+                    sA[s * PT + e] = u0;
+                    sB[(ps.XO + s) * PT + e] = v0;
                 }
-                if (d >= 1) {
-                    const double um = (double)ur[-sh], vm = (double)vr[-sh];
-                    xu += E1[d - 1] * um;
-                    xv += E1[d - 1] * vm;
-                    x3v += E31[d - 1] * vm;
-                }
-                if (d + 2 < nf) {
-                    x2u += E2[d] * (double)ur[2 * sh];
-                    x2v += E2[d] * (double)vr[2 * sh];
-                }
-                if (d >= 2) {
-                    x2u += E2[d - 2] * (double)ur[-2 * sh];
-                    x2v += E2[d - 2] * (double)vr[-2 * sh];
-                }
-                if (d + 3 < nf) x3v += E33[d] * (double)vr[3 * sh];
-                if (d >= 3) x3v += E33[d - 3] * (double)vr[-3 * sh];
+                sA[(S + c) * PT + e] = xu;
+                sA[(S + MS + c) * PT + e] = x2u;
+                sB[c * PT + e] = xv;
+                sB[(ps.XO + S + c) * PT + e] = x2v;
+                sB[(ps.XO + S + MS + c) * PT + e] = ((double)d + 0.5) * v0;
+                sB[(ps.XO + S + 2 * MS + c) * PT + e] = x3v;
             }
-            a[S + k * S + s] = xu;
-            a[S + MS + k * S + s] = x2u;
-            b[S + k * S + s] = xv;
-            b[S + MS + k * S + s] = x2v;
-            b[S + 2 * MS + k * S + s] = hv;
-            b[S + 3 * MS + k * S + s] = x3v;
-        }
-        for (int f = wid; f < S * P2; f += nwarp)
+        } else {
+            const int pd = f - MS, pw = spair[pd], l = pw & 255, m = pw >> 8;
+            const int nl = snf[l], nm = snf[m], shl = ssh[l], shm = ssh[m];
+            double g[RPL][4 * G3_SMAX];
 #pragma unroll
-        for (int hr = 0; hr < G3_TR / 32; ++hr) {
-            const int e = lane + 32 * hr;
-            const long long r = t0 + e;
-            const bool in = r < dimen;
-            double *b = sB + e * nB1;
-            const int s = f / P2, p = f - s * P2, l = spair[p] & 255, m = spair[p] >> 8;
-            double xx = 0.0;
-            if (in) {
-                const T *vr = v + (long long)s * dimen + r;
-                const int dl = sdig[e * M + l], dm = sdig[e * M + m], nl = snf[l], nm = snf[m];
-                const long long shl = ssh[l], shm = ssh[m];
-                const bool lp = dl + 1 < nl, lm = dl >= 1, mp = dm + 1 < nm, mm = dm >= 1;
+            for (int hr = 0; hr < RPL; ++hr) {
+                const int e = lane + 32 * hr;
+                const long long r = t0 + e;
+                const bool in = r < dimen;
+                const int dl = sdig[l * TR + e], dm = sdig[m * TR + e];
+                const bool lp = in && dl + 1 < nl, lm = in && dl >= 1, mp = dm + 1 < nm, mm = dm >= 1;
+                const int opp = lp && mp ? shl + shm : 0, opm = lp && mm ? shl - shm : 0;
+                const int omp = lm && mp ? shm - shl : 0, omm = lm && mm ? -shl - shm : 0;
+                const long long rr = in ? r : t0;
+#pragma unroll
+                for (int s = 0; s < G3_SMAX; ++s)
+                    if (s < S) {
+                        const T *vr = v + (long long)s * dimen + rr;
+                        g[hr][4 * s + 0] = (double)vr[opp];
+                        g[hr][4 * s + 1] = (double)vr[opm];
+                        g[hr][4 * s + 2] = (double)vr[omp];
+                        g[hr][4 * s + 3] = (double)vr[omm];
+                    }
+            }
+            between();
+#pragma unroll
+            for (int hr = 0; hr < RPL; ++hr) {
+                const int e = lane + 32 * hr;
+                const bool in = t0 + e < dimen;
+                const int dl = sdig[l * TR + e], dm = sdig[m * TR + e];
+                const bool lp = in && dl + 1 < nl, lm = in && dl >= 1, mp = dm + 1 < nm, mm = dm >= 1;
                 const double elp = lp ? E1[dl] : 0.0, elm = lm ? E1[dl - 1] : 0.0;
                 const double emp = mp ? E1[dm] : 0.0, emm = mm ? E1[dm - 1] : 0.0;
-                if (lp && mp) xx += elp * emp * (double)vr[shl + shm];
-                if (lp && mm) xx += elp * emm * (double)vr[shl - shm];
-                if (lm && mp) xx += elm * emp * (double)vr[shm - shl];
-                if (lm && mm) xx += elm * emm * (double)vr[-shl - shm];
+                const double cpp = elp * emp, cpm = elp * emm, cmp = elm * emp, cmm = elm * emm;
+#pragma unroll
+                for (int s = 0; s < G3_SMAX; ++s)
+                    if (s < S)
+                        sB[(ps.PO + pd * S + s) * PT + e] =
+                            cpp * g[hr][4 * s] + cpm * g[hr][4 * s + 1] + cmp * g[hr][4 * s + 2] + cmm * g[hr][4 * s + 3];
             }
-            b[S + 4 * MS + p * S + s] = xx;
         }
-        __syncthreads();
-        // Gram sums over the tile's rows: 4 outputs per task, no branches
+    };
+    // MMA steps [k0, k1) (four rows each) of a column tile
+    auto mma = [&](const double *cols, int k0, int k1) {
+        if (nq == 0) return;
+        for (int kk = k0; kk < k1; ++kk)
 #pragma unroll
-        for (int j = 0; j < TPT; ++j) {
-            const double *pa = sA + ia[j];
-            const double *p0 = sB + jb[j][0], *p1 = sB + jb[j][1], *p2 = sB + jb[j][2], *p3 = sB + jb[j][3];
-            double c0 = acc[j][0], c1 = acc[j][1], c2 = acc[j][2], c3 = acc[j][3];
-#pragma unroll 8
-            for (int rr = 0; rr < G3_TR; ++rr) {
-                const double av = pa[rr * nA];
-                c0 += av * p0[rr * nB1];
-                c1 += av * p1[rr * nB1];
-                c2 += av * p2[rr * nB1];
-                c3 += av * p3[rr * nB1];
-            }
-            acc[j][0] = c0;
-            acc[j][1] = c1;
-            acc[j][2] = c2;
-            acc[j][3] = c3;
+            for (int q = 0; q < NBW; ++q)
+                if (q < nq) mma_f64_884(acc[q], cols[aoff[q] + 4 * kk], cols[boff[q] + 4 * kk]);
+    };
+    __syncthreads();  // tables and strides
+    if (ntl > 0) digits(0, sdig0);
+    __syncthreads();
+    if constexpr (NBUF == 2) {
+        // tile i: this warp's families, each followed (while its loads are in flight) by a slice
+        // of the MMA steps of tile i-1; then the digits of tile i+1
+        const int nfam = MS + P2;
+        for (int i = 0; i <= ntl; ++i) {
+            const int nfw = i < ntl && wid < nfam ? (nfam - wid + nwarp - 1) / nwarp : 0;
+            const int nk = i >= 1 ? TR / 4 : 0;
+            const int kc = nfw > 0 ? (nk + nfw - 1) / nfw : nk;
+            const double *mcols = sm + ((i - 1) & 1) * tcols;
+            int kdone = 0;
+            for (int j = 0; j < nfw; ++j)
+                family(wid + j * nwarp, i, sdig0 + (i & 1) * M * TR, sm + (i & 1) * tcols, [&] {
+                    const int k1 = min(nk, kdone + kc);
+                    mma(mcols, kdone, k1);
+                    kdone = k1;
+                });
+            mma(mcols, kdone, nk);
+            if (i + 1 < ntl) digits(i + 1, sdig0 + ((i + 1) & 1) * M * TR);
+            __syncthreads();
         }
-        __syncthreads();
+    } else {
+        for (int i = 0; i < ntl; ++i) {
+            expand(i, sdig0, sm);
+            __syncthreads();
+            mma(sm, 0, TR / 4);
+            if (i + 1 < ntl) digits(i + 1, sdig0);
+            __syncthreads();
+        }
     }
+    // block q's entry (row lane/4, columns 2 (lane%4) + i) at 64 q + 8 row + column
+    double *pb = part + (long long)blockIdx.x * 64 * nblk;
 #pragma unroll
-    for (int j = 0; j < TPT; ++j) {
-        const int t = tid + j * nth;
-        if (t >= ntask) continue;
+    for (int q = 0; q < NBW; ++q)
+        if (q < nq)
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-            if (q < nq[j]) {
-                double *pp = part + (long long)blockIdx.x * nout + 4 * t + q;
-                *pp = accumulate ? *pp + acc[j][q] : acc[j][q];
+            for (int i = 0; i < 2; ++i) {
+                double *pp = pb + (wid * nbw + q) * 64 + (lane >> 2) * 8 + 2 * (lane & 3) + i;
+                *pp = accumulate ? *pp + acc[q][i] : acc[q][i];
             }
-    }
 }
 
-// Column indices of the ordr-3 Gram (host side; the kernel lays them out identically).
 struct G3Cols {
     int S, M, MS, P2, nA, nB;
     G3Cols(int S_, int M_) : S(S_), M(M_), MS(M_ * S_), P2(M_ * (M_ - 1) / 2) {
@@ -551,111 +684,139 @@ struct G3Cols {
     int x3v(int k, int b) const { return S + 3 * MS + k * S + b; }
     int pair(int l, int m) const { return l * M - l * (l + 1) / 2 + (m - l - 1); }  // l < m
     int XXv(int l, int m, int b) const { return S + 4 * MS + pair(l, m) * S + b; }
+    // shared-memory position (G3Pos) of a B column
+    int posB(int jb) const {
+        const G3Pos p(S, M);
+        if (jb < S) return p.XO + jb;                                  // v
+        if (jb < S + MS) return jb - S;                                // X v
+        if (jb < S + 4 * MS) return p.XO + S + (jb - S - MS);          // x^2 v, (n+1/2) v, x^3 v
+        const int q = jb - S - 4 * MS, pr = q / S, b = q - pr * S;     // X_l X_m v: descending l
+        int l = 0;
+        while (pair(l, M - 1) < pr) ++l;
+        const int m = pr - pair(l, l + 1) + l + 1;
+        const int pd = (M - 1 - l) * (M - 2 - l) / 2 + (m - l - 1);
+        return p.PO + pd * S + b;
+    }
 };
 
-// The task list (A column, up to 4 B columns) and the output index of every needed (A, B) pair.
-static void gram3_tasks(int S, int M, std::vector<G3Task> &tasks, std::vector<int> &index) {
+// The needed (A, B) entries of the ordr-3 Gram, the 8 x 8 MMA blocks that hold them (A block
+// | B block << 16, A-block major) and the output index of every needed entry (64 block + 8 row
+// + column; -1 where not formed).
+static void gram3_blocks(int S, int M, std::vector<int> &blocks, std::vector<int> &index) {
     const G3Cols c(S, M);
-    tasks.clear();
-    index.assign((size_t)c.nA * c.nB, -1);
-    // the row's B columns in ascending order, dealt to its K tasks round-robin (task k takes
-    // columns k, k + K, k + 2K, k + 3K): neighbouring threads read neighbouring words of a
-    // shared-memory row (no bank conflicts from a 4-column stride)
-    auto row = [&](int ia, std::vector<int> jbs) {
-        std::sort(jbs.begin(), jbs.end());
-        const int n = (int)jbs.size(), K = (n + 3) / 4, t0 = (int)tasks.size();
-        for (int k = 0; k < K; ++k) {
-            G3Task t{};
-            t.ia = (short)ia;
-            for (int q = 0; q < 4 && k + q * K < n; ++q) {
-                t.jb[q] = (short)jbs[k + q * K];
-                index[(size_t)ia * c.nB + jbs[k + q * K]] = 4 * (t0 + k) + q;
-                t.nq = (short)(q + 1);
-            }
-            tasks.push_back(t);
-        }
-    };
+    const G3Pos p(S, M);
+    std::vector<std::pair<int, int>> need;
     for (int a = 0; a < S; ++a) {
-        std::vector<int> j;
-        for (int b = 0; b < S; ++b) j.push_back(c.v(b));
+        for (int b = 0; b < S; ++b) need.push_back({c.u(a), c.v(b)});
         for (int k = 0; k < M; ++k)
             for (int b = 0; b < S; ++b) {
-                j.push_back(c.Xv(k, b));
-                j.push_back(c.x2v(k, b));
-                j.push_back(c.hv(k, b));
-                j.push_back(c.x3v(k, b));
+                need.push_back({c.u(a), c.Xv(k, b)});
+                need.push_back({c.u(a), c.x2v(k, b)});
+                need.push_back({c.u(a), c.hv(k, b)});
+                need.push_back({c.u(a), c.x3v(k, b)});
             }
-        row(c.u(a), j);
     }
     for (int k = 0; k < M; ++k)
         for (int a = 0; a < S; ++a) {
-            std::vector<int> j;
             for (int l = 0; l < M; ++l)
                 if (l != k)
-                    for (int b = 0; b < S; ++b) j.push_back(c.Xv(l, b));
+                    for (int b = 0; b < S; ++b) {
+                        need.push_back({c.Xu(k, a), c.Xv(l, b)});
+                        need.push_back({c.x2u(k, a), c.Xv(l, b)});
+                    }
             for (int l = k + 1; l < M; ++l)
                 for (int m = l + 1; m < M; ++m)
-                    for (int b = 0; b < S; ++b) j.push_back(c.XXv(l, m, b));
-            row(c.Xu(k, a), j);
-            std::vector<int> j2;
-            for (int l = 0; l < M; ++l)
-                if (l != k)
-                    for (int b = 0; b < S; ++b) j2.push_back(c.Xv(l, b));
-            row(c.x2u(k, a), j2);
+                    for (int b = 0; b < S; ++b) need.push_back({c.Xu(k, a), c.XXv(l, m, b)});
         }
+    const int nbA = p.nA8 / 8, nbB = p.nB8 / 8;
+    std::vector<int> bno((size_t)nbA * nbB, -1);
+    for (auto &e : need) bno[(size_t)(e.first / 8) * nbB + c.posB(e.second) / 8] = 0;
+    blocks.clear();
+    for (int i = 0; i < nbA; ++i)
+        for (int j = 0; j < nbB; ++j)
+            if (bno[(size_t)i * nbB + j] == 0) {
+                bno[(size_t)i * nbB + j] = (int)blocks.size();
+                blocks.push_back(i | (j << 16));
+            }
+    index.assign((size_t)c.nA * c.nB, -1);
+    for (auto &e : need) {
+        const int pb = c.posB(e.second);
+        index[(size_t)e.first * c.nB + e.second] =
+            64 * bno[(size_t)(e.first / 8) * nbB + pb / 8] + 8 * (e.first % 8) + pb % 8;
+    }
 }
 
-static size_t gram3_smem(int S, int M, int nmax) {
-    const G3Cols c(S, M);
-    return (size_t)(G3_TR * (c.nA + c.nB + 1) + 5 * nmax) * sizeof(double) + (size_t)M * sizeof(long long) +
-           (size_t)(G3_TR * M + c.P2 + M) * sizeof(int);
+// Tile shapes in order of preference: TR rows per tile, NBUF column tiles.
+struct G3Shape {
+    int tr, nbuf;
+};
+constexpr G3Shape G3_SHAPES[2] = {{32, 2}, {32, 1}};
+constexpr size_t G3_SMEM_MAX = 200 * 1024;
+
+static size_t gram3_smem(int S, int M, int nmax, G3Shape sh) {
+    const G3Pos p(S, M);
+    const int P2 = M * (M - 1) / 2;
+    return (size_t)(sh.nbuf * (p.nA8 + p.nB8) * (sh.tr + 4) + 5 * nmax) * sizeof(double) +
+           (size_t)(2 * M + P2 + sh.nbuf * sh.tr * M) * sizeof(int);
 }
 
-static bool gram3_fits(int S, int M) {
-    if (M > 255) return false;
-    const G3Cols c(S, M);
-    std::vector<G3Task> t;
-    std::vector<int> idx;
-    if (c.nB > 32767 || c.nA > 32767) return false;
-    gram3_tasks(S, M, t, idx);
-    return gram3_smem(S, M, 64) <= 200 * 1024 && t.size() <= (size_t)4 * G3_THREADS;
+// the first tile shape whose shared memory fits (tr = 0: none)
+static G3Shape gram3_shape(const nvb_handle *h) {
+    for (const G3Shape &sh : G3_SHAPES)
+        if (gram3_smem(h->sys.S, h->sys.M, h->plan.nmax, sh) <= G3_SMEM_MAX) return sh;
+    return {0, 0};
+}
+
+static bool gram3_fits(const nvb_handle *h) {
+    const int S = h->sys.S, M = h->sys.M;
+    if (M > 255 || M < 1 || S > G3_SMAX || h->sys.dimen > 0x7fffffffll) return false;
+    if (gram3_shape(h).tr == 0) return false;
+    std::vector<int> b, idx;
+    gram3_blocks(S, M, b, idx);
+    return b.size() <= (size_t)G3_NBW * (G3_THREADS / 32);
 }
 
 static int gram3_len(int S, int M) {
-    std::vector<G3Task> t;
-    std::vector<int> idx;
-    gram3_tasks(S, M, t, idx);
-    return 4 * (int)t.size();
-}
-
-// the task table on the device and the grid, once per handle
-static void gram3_setup(nvb_handle *h) {
-    if (h->d_g3task) return;
-    std::vector<G3Task> t;
-    std::vector<int> idx;
-    gram3_tasks(h->sys.S, h->sys.M, t, idx);
-    CK(cudaMalloc(&h->d_g3task, t.size() * sizeof(G3Task)));
-    CK(cudaMemcpy(h->d_g3task, t.data(), t.size() * sizeof(G3Task), cudaMemcpyHostToDevice));
-    h->g3_ntask = (int)t.size();
-    int nsm = 0;
-    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
-    h->g3_grid = (int)std::min<long long>((h->sys.dimen + G3_TR - 1) / G3_TR, (long long)nsm * 2);
+    std::vector<int> b, idx;
+    gram3_blocks(S, M, b, idx);
+    return 64 * (int)b.size();
 }
 
 static int gram3_grid(const nvb_handle *h) {
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
-    return (int)std::min<long long>((h->sys.dimen + G3_TR - 1) / G3_TR, (long long)nsm * 2);
+    const int tr = gram3_shape(h).tr;
+    return (int)std::min<long long>((h->sys.dimen + tr - 1) / tr, (long long)nsm * 2);
 }
 
-template <typename T, int TPT>
-static void gram3_kernel(nvb_handle *h, const T *u, const T *v, int accumulate, double *part, size_t shm) {
-    auto k = k_adj_gram3<T, TPT>;
+// the block list on the device and the grid, once per handle
+static void gram3_setup(nvb_handle *h) {
+    if (h->d_g3blk) return;
+    std::vector<int> b, idx;
+    gram3_blocks(h->sys.S, h->sys.M, b, idx);
+    CK(cudaMalloc(&h->d_g3blk, b.size() * sizeof(int)));
+    CK(cudaMemcpy(h->d_g3blk, b.data(), b.size() * sizeof(int), cudaMemcpyHostToDevice));
+    h->g3_nblk = (int)b.size();
+    h->g3_grid = gram3_grid(h);
+}
+
+template <typename T, int TR, int NBW, int NBUF>
+static void gram3_kernel(nvb_handle *h, const T *u, const T *v, int nbw, int accumulate, double *part, size_t shm) {
+    auto k = k_adj_gram3<T, TR, NBW, NBUF>;
     if (shm > 48 * 1024) CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     const Plan &pl = h->plan;
     k<<<h->g3_grid, G3_THREADS, shm, h->stream>>>(u, v, pl.d_etab, pl.nmax, pl.d_nfunc, pl.d_shft, h->sys.M, h->sys.S,
-                                                   h->sys.dimen, (const G3Task *)h->d_g3task, h->g3_ntask,
+                                                   h->sys.dimen, (const int *)h->d_g3blk, h->g3_nblk, nbw,
                                                    accumulate, part);
+}
+
+template <typename T, int TR, int NBUF>
+static void gram3_kernel_nbw(nvb_handle *h, const T *u, const T *v, int nbw, int accumulate, double *part,
+                             size_t shm) {
+    if (nbw <= 2) gram3_kernel<T, TR, 2, NBUF>(h, u, v, nbw, accumulate, part, shm);
+    else if (nbw <= 4) gram3_kernel<T, TR, 4, NBUF>(h, u, v, nbw, accumulate, part, shm);
+    else if (nbw <= 6) gram3_kernel<T, TR, 6, NBUF>(h, u, v, nbw, accumulate, part, shm);
+    else gram3_kernel<T, TR, 8, NBUF>(h, u, v, nbw, accumulate, part, shm);
 }
 
 // G (+)= the ordr-3 Gram entries of (u, v) through block partials part[g3_grid * gram3_len];
@@ -663,19 +824,15 @@ static void gram3_kernel(nvb_handle *h, const T *u, const T *v, int accumulate, 
 template <typename T>
 static void gram3_launch(nvb_handle *h, const T *u, const T *v, double *G, int accumulate, double *part) {
     const int S = h->sys.S, M = h->sys.M;
-    if (!gram3_fits(S, M)) fail(NVB_ERR_ARG, "adjoint: too many modes x states for the ordr-3 Gram path");
+    if (!gram3_fits(h)) fail(NVB_ERR_ARG, "adjoint: too many modes x states for the ordr-3 Gram path");
     gram3_setup(h);
-    const size_t shm = gram3_smem(S, M, h->plan.nmax);
-    if (shm > 227 * 1024) fail(NVB_ERR_ARG, "adjoint: the ordr-3 Gram tile does not fit in shared memory");
-    const int tpt = (h->g3_ntask + G3_THREADS - 1) / G3_THREADS;
+    const G3Shape sh = gram3_shape(h);
+    const size_t shm = gram3_smem(S, M, h->plan.nmax, sh);
+    const int nwarp = G3_THREADS / 32, nbw = (h->g3_nblk + nwarp - 1) / nwarp;
     const int acc = G ? 0 : accumulate;
-    switch (tpt) {
-    case 1: gram3_kernel<T, 1>(h, u, v, acc, part, shm); break;
-    case 2: gram3_kernel<T, 2>(h, u, v, acc, part, shm); break;
-    case 3: gram3_kernel<T, 3>(h, u, v, acc, part, shm); break;
-    default: gram3_kernel<T, 4>(h, u, v, acc, part, shm); break;
-    }
-    const int nout = 4 * h->g3_ntask;
+    if (sh.nbuf == 2) gram3_kernel_nbw<T, 32, 2>(h, u, v, nbw, acc, part, shm);
+    else gram3_kernel_nbw<T, 32, 1>(h, u, v, nbw, acc, part, shm);
+    const int nout = 64 * h->g3_nblk;
     if (G) k_gram_reduce<<<(nout * 32 + 255) / 256, 256, 0, h->stream>>>(part, h->g3_grid, nout, accumulate, G);
     CK(cudaGetLastError());
 }
@@ -783,14 +940,14 @@ static void gram_pc(const nvb_handle *h, const std::vector<double> &Gh, const st
 }
 
 // P[m][a][b] for the monomials of an ordr-3 system and Cq = (C[a][b], K_k) from the Gram
-// entries (host copy Gh of length gram3_len, laid out by gram3_tasks)
+// entries (host copy Gh of length gram3_len, laid out by gram3_blocks)
 static void gram3_pc(const nvb_handle *h, const std::vector<double> &Gh, const std::vector<Mono> &monos,
                      std::vector<double> &P, std::vector<double> &Cq) {
     const int S = h->sys.S, M = h->sys.M;
     const G3Cols c(S, M);
-    std::vector<G3Task> tasks;
+    std::vector<int> blocks;
     std::vector<int> index;
-    gram3_tasks(S, M, tasks, index);
+    gram3_blocks(S, M, blocks, index);
     auto G = [&](int ia, int jb) {
         const int o = index[(size_t)ia * c.nB + jb];
         if (o < 0) fail(NVB_ERR_STATE, "adjoint: Gram entry not formed");
@@ -834,7 +991,7 @@ template <typename T>
 static void gram3_adjoint(nvb_handle *h, const T *u, const T *v, const std::vector<Mono> &monos, std::vector<double> &P,
                           std::vector<double> &Cq) {
     gram3_setup(h);
-    const int nout = 4 * h->g3_ntask, grid = h->g3_grid;
+    const int nout = 64 * h->g3_nblk, grid = h->g3_grid;
     double *part = (double *)scratch_vector(h, ((size_t)grid + 1) * nout * sizeof(double));
     double *G = part + (size_t)grid * nout;
     gram3_launch<T>(h, u, v, G, 0, part);
@@ -928,7 +1085,7 @@ static void adjoint_s(nvb_handle *h, const T *u, const T *v, double *grad) {
     std::vector<double> Cq;
     if (sys.ordr <= 2 && gram_fits(S, M)) {
         gram_adjoint<T>(h, u, v, monos, P, Cq);
-    } else if (sys.ordr == 3 && gram3_fits(S, M)) {
+    } else if (sys.ordr == 3 && gram3_fits(h)) {
         gram3_adjoint<T>(h, u, v, monos, P, Cq);
     } else {
     double *part = nullptr;
@@ -1012,7 +1169,7 @@ void hv_adjoint(nvb_handle *h, const void *u, const void *v, int dtype, double *
 // Accumulated adjoint for the reverse sweep (ordr <= 2 systems whose Gram matrices fit): the
 // gradient is linear in the Gram matrices, so the sweep sums them on the device over all
 // steps and assembles the gradient once.
-static bool gram3_path(const nvb_handle *h) { return h->sys.ordr == 3 && gram3_fits(h->sys.S, h->sys.M); }
+static bool gram3_path(const nvb_handle *h) { return h->sys.ordr == 3 && gram3_fits(h); }
 
 int64_t adjoint_gram_len(const nvb_handle *h) {
     if (h->sys.ordr <= 2 && gram_fits(h->sys.S, h->sys.M)) return gram_len(h->sys.S, h->sys.M);

@@ -191,7 +191,7 @@ int nvb_destroy(nvb_handle *h) {
             slab_free(h->slab[0]);
             slab_free(h->slab[1]);
             quad_free(h->quad);
-            if (h->d_g3task) cudaFree(h->d_g3task);
+            if (h->d_g3blk) cudaFree(h->d_g3blk);
             cubic_free(h->cubic);
             ckpt_free(h);
             if (h->seed_vec) cudaFree(h->seed_vec);

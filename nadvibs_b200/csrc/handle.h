@@ -21,9 +21,9 @@ struct nvb_handle {
     nvb::SlabPlan slab[2];  // slab-tiled H.v plans for FP64 (0) and FP32 (1) vectors
     nvb::QuadPlan quad;     // factorised quadratic H.v plan (both precisions)
     nvb::CubPlan cubic;     // factorised cubic H.v plan (both precisions)
-    // ordr-3 Gram adjoint (adjoint.cu): its task table on the device, task count and grid
-    void *d_g3task = nullptr;
-    int g3_ntask = 0, g3_grid = 0;
+    // ordr-3 Gram adjoint (adjoint.cu): its 8 x 8 MMA block list on the device, block count and grid
+    void *d_g3blk = nullptr;
+    int g3_nblk = 0, g3_grid = 0;
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;

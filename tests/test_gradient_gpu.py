@@ -114,3 +114,43 @@ def test_hellmann_feynman_matches_dense_eigenvalue_derivative():
         tm[i] -= h_i
         fd = (lowest(tp) - lowest(tm)) / (2 * h_i)
         assert G[0, i] == pytest.approx(fd, rel=1e-5, abs=1e-9 * max(1.0, abs(fd)))
+
+
+def test_adjoint_cubic_eleven_modes_single_buffered_tile():
+    """3 states and 11 modes give 384 Gram columns: too many for two column tiles in shared
+    memory, so the cubic Gram path runs its single-buffered tile.  Checked against central
+    differences of the oracle on every frequency and block constant and a spread of expansion
+    coefficients of each degree."""
+    nstates, basis, ordr, seed = 3, [2, 2, 3, 2, 2, 2, 2, 2, 2, 3, 2], 3, 49
+    cfg = synth.random_small(seed, nstates, basis, ordr)
+    om, cc, pot = synth.draw_small(cfg)
+    M = len(basis)
+    nb = nstates * (nstates + 1) // 2
+    potf = synth.flatten_pot(pot)
+    npot = len(potf)
+    theta = np.concatenate([potf, cc, om])
+    S = O.system_from_arrays(basis, nstates, ordr, om, cc, pot, quirk_lower=False, quirk_cubic=True)
+    rng = np.random.default_rng(seed)
+    u = rng.normal(size=S.ntotal)
+    v = rng.normal(size=S.ntotal)
+    with L.Handle.from_arrays(_params(nstates, basis, ordr), om, cc, potf, quirk_lower=0, quirk_cubic=1) as h:
+        ut = torch.from_numpy(u).to("cuda")
+        vt = torch.from_numpy(v).to("cuda")
+        torch.cuda.synchronize()
+        g = h.adjoint_ptr(ut.data_ptr(), vt.data_ptr(), L.DTYPE_F64)
+
+    def f(th):
+        w, c, p = _split(th, npot, nb, M)
+        Sx = O.system_from_arrays(basis, nstates, ordr, w, c, _unflatten(p, nb, ordr, M), quirk_lower=False,
+                                  quirk_cubic=True, ztoler=0.0)
+        return float(u @ Sx.hv(v))
+
+    idx = list(range(0, npot, 23)) + list(range(npot, len(theta)))
+    fd = np.zeros(len(idx))
+    for j, i in enumerate(idx):
+        h_i = 1e-6 * max(abs(theta[i]), 1e-3)
+        tp, tm = theta.copy(), theta.copy()
+        tp[i] += h_i
+        tm[i] -= h_i
+        fd[j] = (f(tp) - f(tm)) / (2 * h_i)
+    assert np.abs(g[idx] - fd).max() <= 1e-6 * np.abs(fd).max()
