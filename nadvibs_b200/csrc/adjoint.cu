@@ -371,13 +371,15 @@ __device__ __forceinline__ void mma_f64_884(double (&c)[2], double a, double b) 
 // NBUF = 2: two column tiles, so one barrier per tile separates the expansion of tile i (and the
 // digits of tile i+1) from the MMAs of tile i-1, and warps in either phase overlap; NBUF = 1:
 // one tile, expansion and MMAs separated by barriers.
-template <typename T, int TR, int NBW, int NBUF>
+template <typename T, int TR, int NBW, int NBUF, int S>
 __global__ void __launch_bounds__(G3_THREADS, 1)
     k_adj_gram3(const T *__restrict__ u, const T *__restrict__ v, const double *__restrict__ etab, int nmax,
-                const int *__restrict__ nfunc, const long long *__restrict__ shft, int M, int S, long long dimen,
+                const int *__restrict__ nfunc, const long long *__restrict__ shft, int M, long long dimen,
                 const int *__restrict__ blocks, int nblk, int nbw, int accumulate, double *__restrict__ part) {
     constexpr int PT = TR + 4, RPL = TR / 32;
     static_assert(TR % 32 == 0, "whole warps of rows");
+    static_assert(S >= 1 && S <= G3_SMAX, "states");
+    const int dimi = (int)dimen;  // <= INT_MAX (checked on the host)
     extern __shared__ double sm[];
     const int MS = M * S, P2 = M * (M - 1) / 2;
     const G3Pos ps(S, M);
@@ -516,20 +518,20 @@ __global__ void __launch_bounds__(G3_THREADS, 1)
     // clamped to the row itself and their coefficients are zero, so the loads are unconditional.
     auto family = [&](int f, int t, const int *sdig, double *sA, auto &&between) {
         double *sB = sA + ps.nA8 * PT;
-        const long long t0 = first + (long long)t * tstride;  // < dimen: the tile exists
+        const int t0 = (int)(first + (long long)t * tstride);  // < dimen <= INT_MAX: the tile exists
         if (f < MS) {
             const int k = f / S, s = f - k * S, nf = snf[k], sh = ssh[k];
             double g[RPL][12];
 #pragma unroll
             for (int hr = 0; hr < RPL; ++hr) {
                 const int e = lane + 32 * hr;
-                const long long r = t0 + e;
-                const bool in = r < dimen;
+                const int r = t0 + e;
+                const bool in = r < dimi;
                 const int d = sdig[k * TR + e];
                 const int o1p = in && d + 1 < nf ? sh : 0, o1m = in && d >= 1 ? -sh : 0;
                 const int o2p = in && d + 2 < nf ? 2 * sh : 0, o2m = in && d >= 2 ? -2 * sh : 0;
                 const int o3p = in && d + 3 < nf ? 3 * sh : 0, o3m = in && d >= 3 ? -3 * sh : 0;
-                const long long rr = in ? r : t0;
+                const int rr = in ? r : t0;
                 const T *ur = u + (long long)s * dimen + rr, *vr = v + (long long)s * dimen + rr;
                 g[hr][0] = (double)ur[0];
                 g[hr][1] = (double)vr[0];
@@ -548,7 +550,7 @@ __global__ void __launch_bounds__(G3_THREADS, 1)
 #pragma unroll
             for (int hr = 0; hr < RPL; ++hr) {
                 const int e = lane + 32 * hr;
-                const bool in = t0 + e < dimen;
+                const bool in = t0 + e < dimi;
                 const int d = sdig[k * TR + e];
                 const bool p1 = in && d + 1 < nf, m1 = in && d >= 1, p2 = in && d + 2 < nf, m2 = in && d >= 2;
                 const bool p3 = in && d + 3 < nf, m3 = in && d >= 3;
@@ -581,13 +583,13 @@ __global__ void __launch_bounds__(G3_THREADS, 1)
 #pragma unroll
             for (int hr = 0; hr < RPL; ++hr) {
                 const int e = lane + 32 * hr;
-                const long long r = t0 + e;
-                const bool in = r < dimen;
+                const int r = t0 + e;
+                const bool in = r < dimi;
                 const int dl = sdig[l * TR + e], dm = sdig[m * TR + e];
                 const bool lp = in && dl + 1 < nl, lm = in && dl >= 1, mp = dm + 1 < nm, mm = dm >= 1;
                 const int opp = lp && mp ? shl + shm : 0, opm = lp && mm ? shl - shm : 0;
                 const int omp = lm && mp ? shm - shl : 0, omm = lm && mm ? -shl - shm : 0;
-                const long long rr = in ? r : t0;
+                const int rr = in ? r : t0;
 #pragma unroll
                 for (int s = 0; s < G3_SMAX; ++s)
                     if (s < S) {
@@ -602,7 +604,7 @@ __global__ void __launch_bounds__(G3_THREADS, 1)
 #pragma unroll
             for (int hr = 0; hr < RPL; ++hr) {
                 const int e = lane + 32 * hr;
-                const bool in = t0 + e < dimen;
+                const bool in = t0 + e < dimi;
                 const int dl = sdig[l * TR + e], dm = sdig[m * TR + e];
                 const bool lp = in && dl + 1 < nl, lm = in && dl >= 1, mp = dm + 1 < nm, mm = dm >= 1;
                 const double elp = lp ? E1[dl] : 0.0, elm = lm ? E1[dl - 1] : 0.0;
@@ -800,23 +802,30 @@ static void gram3_setup(nvb_handle *h) {
     h->g3_grid = gram3_grid(h);
 }
 
-template <typename T, int TR, int NBW, int NBUF>
+template <typename T, int TR, int NBW, int NBUF, int S>
 static void gram3_kernel(nvb_handle *h, const T *u, const T *v, int nbw, int accumulate, double *part, size_t shm) {
-    auto k = k_adj_gram3<T, TR, NBW, NBUF>;
+    auto k = k_adj_gram3<T, TR, NBW, NBUF, S>;
     if (shm > 48 * 1024) CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     const Plan &pl = h->plan;
-    k<<<h->g3_grid, G3_THREADS, shm, h->stream>>>(u, v, pl.d_etab, pl.nmax, pl.d_nfunc, pl.d_shft, h->sys.M, h->sys.S,
+    k<<<h->g3_grid, G3_THREADS, shm, h->stream>>>(u, v, pl.d_etab, pl.nmax, pl.d_nfunc, pl.d_shft, h->sys.M,
                                                    h->sys.dimen, (const int *)h->d_g3blk, h->g3_nblk, nbw,
                                                    accumulate, part);
 }
 
-template <typename T, int TR, int NBUF>
+template <typename T, int TR, int NBUF, int S>
 static void gram3_kernel_nbw(nvb_handle *h, const T *u, const T *v, int nbw, int accumulate, double *part,
                              size_t shm) {
-    if (nbw <= 2) gram3_kernel<T, TR, 2, NBUF>(h, u, v, nbw, accumulate, part, shm);
-    else if (nbw <= 4) gram3_kernel<T, TR, 4, NBUF>(h, u, v, nbw, accumulate, part, shm);
-    else if (nbw <= 6) gram3_kernel<T, TR, 6, NBUF>(h, u, v, nbw, accumulate, part, shm);
-    else gram3_kernel<T, TR, 8, NBUF>(h, u, v, nbw, accumulate, part, shm);
+    if (nbw <= 2) gram3_kernel<T, TR, 2, NBUF, S>(h, u, v, nbw, accumulate, part, shm);
+    else if (nbw <= 4) gram3_kernel<T, TR, 4, NBUF, S>(h, u, v, nbw, accumulate, part, shm);
+    else if (nbw <= 6) gram3_kernel<T, TR, 6, NBUF, S>(h, u, v, nbw, accumulate, part, shm);
+    else gram3_kernel<T, TR, 8, NBUF, S>(h, u, v, nbw, accumulate, part, shm);
+}
+
+template <typename T, int S>
+static void gram3_kernel_s(nvb_handle *h, const T *u, const T *v, int nbuf, int nbw, int accumulate, double *part,
+                           size_t shm) {
+    if (nbuf == 2) gram3_kernel_nbw<T, 32, 2, S>(h, u, v, nbw, accumulate, part, shm);
+    else gram3_kernel_nbw<T, 32, 1, S>(h, u, v, nbw, accumulate, part, shm);
 }
 
 // G (+)= the ordr-3 Gram entries of (u, v) through block partials part[g3_grid * gram3_len];
@@ -830,8 +839,12 @@ static void gram3_launch(nvb_handle *h, const T *u, const T *v, double *G, int a
     const size_t shm = gram3_smem(S, M, h->plan.nmax, sh);
     const int nwarp = G3_THREADS / 32, nbw = (h->g3_nblk + nwarp - 1) / nwarp;
     const int acc = G ? 0 : accumulate;
-    if (sh.nbuf == 2) gram3_kernel_nbw<T, 32, 2>(h, u, v, nbw, acc, part, shm);
-    else gram3_kernel_nbw<T, 32, 1>(h, u, v, nbw, acc, part, shm);
+    switch (S) {
+    case 1: gram3_kernel_s<T, 1>(h, u, v, sh.nbuf, nbw, acc, part, shm); break;
+    case 2: gram3_kernel_s<T, 2>(h, u, v, sh.nbuf, nbw, acc, part, shm); break;
+    case 3: gram3_kernel_s<T, 3>(h, u, v, sh.nbuf, nbw, acc, part, shm); break;
+    default: gram3_kernel_s<T, 4>(h, u, v, sh.nbuf, nbw, acc, part, shm); break;
+    }
     const int nout = 64 * h->g3_nblk;
     if (G) k_gram_reduce<<<(nout * 32 + 255) / 256, 256, 0, h->stream>>>(part, h->g3_grid, nout, accumulate, G);
     CK(cudaGetLastError());
