@@ -289,7 +289,7 @@ int nvb_seed_overlap(nvb_handle *h, double *overlap);
 /* Record checkpoints of the forward for nvb_lanczos_backward: from the next nvb_seed on,
  * nvb_lanczos saves (v_{c-1}, v_c) at iterations c = 1, 1+k, 1+2k, ... in device memory
  * (2 ceil(niter/k) vectors of the handle's precision).  k = -1 records the whole forward
- * (every v_j and w_j = H v_j, 2 niter + 2 vectors) when that and the sweep's work vectors fit
+ * (every v_j, niter + 2 vectors) when that and the sweep's work vectors fit
  * the budget of nvb_set_backward_memory, and nothing otherwise; a sweep with k = -1 then
  * replays nothing (or, without the record, takes the automatic plan of k = 0).  k = 0 stops
  * recording and frees them.  No reference counterpart. */
@@ -302,15 +302,17 @@ int nvb_set_checkpoints(nvb_handle *h, int64_t k);
  * replaying the recurrence from checkpoint pairs (v_{c-1}, v_c):
  *   k > 0: one level, pairs every k iterations (the forward's, when nvb_set_checkpoints(h, k)
  *          preceded nvb_seed; else one replay from the seed records them), each range of k
- *          iterations replayed into storage (2k + 3 vectors of the handle's precision);
+ *          iterations replayed into storage (k + 2 vectors of the handle's precision);
  *   k = -1: the forward's full record (nvb_set_checkpoints(h, -1)), nothing replayed; the
  *          automatic plan when the record was not kept;
  *   k = 0: automatic.  The shallowest recursion that fits the budget of
  *          nvb_set_backward_memory (default 85% of free device memory): with depth L, each
  *          level splits its range into B ~ n^(1/(L+1)) sub-ranges whose starting pairs one
  *          replay records, down to ranges of at most B iterations replayed into storage
- *          (2 L B + 2 B + 3 vectors; L + 1 replays of the run).  L = 0 (everything stored,
- *          2n + 3 vectors) when it fits.  The forward's pairs, when recorded, are the top level.
+ *          (2 L B + B + 2 vectors; L + 1 replays of the run).  L = 0 (everything stored,
+ *          n + 2 vectors) when it fits.  The forward's pairs, when recorded, are the top level.
+ * No plan stores w_j = H v_j: each step rebuilds it from the recurrence,
+ * w_j = beta_j v_{j+1} + alpha_j v_j + beta_{j-1} v_{j-1}, from the same stored vectors.
  * Adjoint vectors and dot products are FP64 in every plan; the gradient does not depend on the
  * plan beyond rounding of FP64 sums.  Needs H^T = H (fails with NVB_ERR_STATE under
  * quirk_lower with inter-state constant or even-power couplings).  No reference counterpart

@@ -18,13 +18,15 @@
 // The primal vectors come back range by range, last range first, by replaying the recurrence
 // with the stored alpha/beta in the handle's precision (the way the two-pass Ritz vectors are
 // rebuilt) from checkpoint pairs (v_{c-1}, v_c).  A range of at most bmax iterations is
-// replayed into storage (v_{c-1}..v_{e+1} and w_j = H v_j, native precision) and reversed; a
-// longer range is split into up to B sub-ranges, one replay records their starting pairs, and
-// they are reversed last-first (recursive checkpointing).  With an explicit interval k there is
-// one level: pairs every k iterations (the forward's, nvb_set_checkpoints) and bmax = k.  With
-// k = 0 the shallowest depth L that fits the memory budget is used (B = bmax ~ n^(1/(L+1)),
-// 2 L B + 2 bmax + 3 native vectors, L + 1 replays of the run).  The adjoint vectors and every
-// dot product are FP64 (10 FP64 work vectors).
+// replayed into storage (v_{c-1}..v_{e+1}, native precision) and reversed; a longer range is
+// split into up to B sub-ranges, one replay records their starting pairs, and they are reversed
+// last-first (recursive checkpointing).  With an explicit interval k there is one level: pairs
+// every k iterations (the forward's, nvb_set_checkpoints) and bmax = k.  With k = 0 the
+// shallowest depth L that fits the memory budget is used (B = bmax ~ n^(1/(L+1)),
+// 2 L B + bmax + 2 native vectors, L + 1 replays of the run).  No w_j = H v_j is stored: the
+// step rebuilds it from the recurrence, w_j = beta_j v_{j+1} + alpha_j v_j + beta_{j-1} v_{j-1},
+// from the same stored vectors in every plan (so every plan gives the same gradient).  The
+// adjoint vectors and every dot product are FP64 (10 FP64 work vectors).
 //
 // A reverse step does not synchronise with the host: its dot products and bbar stay in device
 // memory and feed the step kernels directly, and for systems with the Gram path (ordr <= 2)
@@ -90,6 +92,19 @@ __global__ void k_lin(double *__restrict__ out, double a1, const double *__restr
     }
 }
 
+// w_i = H v_i rebuilt from the recurrence: r_i = w_i - alpha_i v_i - beta_{i-1} v_{i-1} and
+// v_{i+1} = r_i / beta_i give w_i = beta_i v_{i+1} + alpha_i v_i + beta_{i-1} v_{i-1}
+// (cn, cp carry the scales of the stored vectors; vp null for i = 1, where v_0 = 0)
+__global__ void k_wrec(double *__restrict__ w, double cn, const double *__restrict__ vn, double al,
+                       const double *__restrict__ vi, double cp, const double *__restrict__ vp, long long n) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        double v = cn * vn[i] + al * vi[i];
+        if (vp) v += cp * vp[i];
+        w[i] = v;
+    }
+}
+
 // the replay step of the two-pass Ritz vectors: w = w - alpha sc c - beta_prev sp p
 template <typename T>
 __global__ void k_replay(T *__restrict__ w, const T *__restrict__ c, const T *__restrict__ p, double sc, double sp,
@@ -152,16 +167,16 @@ struct DevBuf {
 
 static void rec_free(nvb_handle *h) {
     if (h->rec_v) cudaFree(h->rec_v);
-    if (h->rec_w) cudaFree(h->rec_w);
     if (h->rec_vs) cudaFree(h->rec_vs);
-    h->rec_v = h->rec_w = nullptr;
+    h->rec_v = nullptr;
     h->rec_vs = nullptr;
     h->rec_cap = h->rec_n = 0;
     h->rec_ok = false;
 }
 
-// The full record (ck_k = -1) for iterations 1..total_iters, from the seed: kept only when it
-// and the sweep's FP64 work vectors fit the backward budget (nvb_set_backward_memory, default
+// The full record (ck_k = -1) of v_0..v_{total_iters+1}, from the seed (w_j = H v_j is rebuilt
+// from them in the sweep): kept only when it and the sweep's FP64 work vectors fit the backward
+// budget (nvb_set_backward_memory, default
 // 85 % of the free device memory); otherwise nothing is recorded and the sweep replays.
 static void rec_reserve(nvb_handle *h, int64_t total_iters) {
     if (h->iters == 0) h->rec_n = 0;
@@ -174,23 +189,21 @@ static void rec_reserve(nvb_handle *h, int64_t total_iters) {
     const size_t keep = h->rec_ok ? (size_t)h->rec_n : 0;
     size_t freeb = 0, totalb = 0;
     CK(cudaMemGetInfo(&freeb, &totalb));
-    const double held = h->rec_ok ? (double)(2 * h->rec_cap + 2) * (double)per : 0.0;
+    const double held = h->rec_ok ? (double)(h->rec_cap + 2) * (double)per : 0.0;
     const double budget = h->grad_budget > 0 ? (double)h->grad_budget : 0.85 * ((double)freeb + held);
-    const double need = (double)(2 * total_iters + 2) * (double)per + (sweep_hv_f32(h) ? 7.0 : 5.0) * (double)per +
+    const double need = (double)(total_iters + 2) * (double)per + (sweep_hv_f32(h) ? 7.0 : 5.0) * (double)per +
                         10.0 * (double)per64;
     if (need > budget) {
         rec_free(h);
         return;
     }
-    void *nv = nullptr, *nw = nullptr;
+    void *nv = nullptr;
     double *ns = nullptr;
     bool ok = cudaMalloc(&nv, (size_t)(total_iters + 2) * per) == cudaSuccess &&
-              cudaMalloc(&nw, (size_t)std::max<int64_t>(total_iters, 1) * per) == cudaSuccess &&
               cudaMalloc((void **)&ns, (size_t)(total_iters + 2) * sizeof(double)) == cudaSuccess;
     if (!ok) {
         (void)cudaGetLastError();  // an out-of-memory return is not sticky: clear it, record nothing
         if (nv) cudaFree(nv);
-        if (nw) cudaFree(nw);
         if (ns) cudaFree(ns);
         rec_free(h);
         return;
@@ -200,7 +213,6 @@ static void rec_reserve(nvb_handle *h, int64_t total_iters) {
     if (keep > 0) {
         CK(cudaMemcpyAsync((char *)nv + per, (char *)h->rec_v + per, (keep + 1) * per, cudaMemcpyDeviceToDevice,
                            h->stream));
-        CK(cudaMemcpyAsync(nw, h->rec_w, keep * per, cudaMemcpyDeviceToDevice, h->stream));
         CK(cudaMemcpyAsync(ns + 1, h->rec_vs + 1, (keep + 1) * sizeof(double), cudaMemcpyDeviceToDevice,
                            h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -208,15 +220,14 @@ static void rec_reserve(nvb_handle *h, int64_t total_iters) {
     const int64_t n_keep = (int64_t)keep;
     rec_free(h);
     h->rec_v = nv;
-    h->rec_w = nw;
     h->rec_vs = ns;
     h->rec_cap = total_iters;
     h->rec_n = n_keep;
     h->rec_ok = true;
 }
 
-// At the start of iteration it (buffers cur = v_it with its scale) and after its H.v (work =
-// w_it): the full record's copies.  At the end of a run, v_{it+1}.
+// At the start of iteration it (buffer cur = v_it with its scale): the full record's copy; after
+// its H.v the record counts iteration it as done.  At the end of a run, v_{it+1}.
 void rec_save_v(nvb_handle *h, int64_t it) {
     if (h->ck_k != -1 || !h->rec_ok || it > h->rec_cap + 1 || h->rec_n < it - 1) return;
     const size_t per = (size_t)h->ntotal() * h->elem_size();
@@ -224,11 +235,8 @@ void rec_save_v(nvb_handle *h, int64_t it) {
     CK(cudaMemcpyAsync(h->rec_vs + it, h->d_scale + h->cur, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
 }
 
-void rec_save_w(nvb_handle *h, int64_t it) {
+void rec_done(nvb_handle *h, int64_t it) {
     if (h->ck_k != -1 || !h->rec_ok || it > h->rec_cap || h->rec_n != it - 1) return;
-    const size_t per = (size_t)h->ntotal() * h->elem_size();
-    CK(cudaMemcpyAsync((char *)h->rec_w + (size_t)(it - 1) * per, h->buf[h->work], per, cudaMemcpyDeviceToDevice,
-                       h->stream));
     h->rec_n = it;
 }
 
@@ -359,7 +367,7 @@ struct Sweep {
     int dt = NVB_DTYPE_F64, g = 1;
     int64_t n = 0, B = 2, bmax = 1;  // branching of a level, longest range reversed from storage
     void *b3[3] = {nullptr, nullptr, nullptr};
-    void *segv = nullptr, *segw = nullptr;  // native v_{c-1}..v_{e+1} and w_c..w_e of a base range
+    void *segv = nullptr;                    // native v_{c-1}..v_{e+1} of a base range
     std::vector<double> segs;                // their scales
     double *vb_next = nullptr, *vb_cur = nullptr, *vb_prev = nullptr, *rbar = nullptr, *wbar = nullptr,
            *wv = nullptr, *v64[3] = {nullptr, nullptr, nullptr}, *w64 = nullptr;
@@ -417,20 +425,19 @@ struct Sweep {
         }
     }
 
-    // reverse steps e..c of a range whose v_{c-1}..v_{e+1} and w_c..w_e are in segv/segw
+    // reverse steps e..c of a range whose v_{c-1}..v_{e+1} are in segv (w_i rebuilt from them)
     void reverse_steps(int64_t c, int64_t e) {
         auto V = [&](int64_t j, double *dst) { to64(dst, nat(segv, j - (c - 1)), segs[j - (c - 1)]); };
         for (int64_t i = e; i >= c; --i) {
             const double al = h->alpha[i], be = h->beta[i], bprev = h->beta[i - 1];
-            // v_{i+1}, v_{i-1} and w_i are read where they are stored (FP64 handles: the stored
-            // vector and its scale, no copy); v_i, which the adjoint contraction also reads,
-            // and everything of a mixed handle are widened to FP64 first
+            // v_{i+1} and v_{i-1} are read where they are stored (FP64 handles: the stored vector
+            // and its scale, no copy); v_i, which the adjoint contraction also reads, and
+            // everything of a mixed handle are widened to FP64 first
             const double *vn = v64[0], *vp = v64[2], *wi = w64, *vi = v64[1];
             double sn = 1.0, sp = 1.0;
             if (mixed) {
                 V(i + 1, v64[0]);
                 if (i > 1) V(i - 1, v64[2]);
-                to64(w64, nat(segw, i - c), 1.0);  // w_i = H v_i from the replay
             } else {
                 vn = (const double *)nat(segv, i + 1 - (c - 1));
                 sn = segs[i + 1 - (c - 1)];
@@ -438,9 +445,9 @@ struct Sweep {
                     vp = (const double *)nat(segv, i - 1 - (c - 1));
                     sp = segs[i - 1 - (c - 1)];
                 }
-                wi = (const double *)nat(segw, i - c);
             }
             V(i, v64[1]);
+            k_wrec<<<g, 256, 0, h->stream>>>(w64, be * sn, vn, al, vi, bprev * sp, i > 1 ? vp : nullptr, N);
             device_dot_async(h, vb_next, 1.0, vn, sn, NVB_DTYPE_F64, d_dots);
             k_rbar<<<g, 256, 0, h->stream>>>(rbar, vb_next, vn, sn, 1.0 / be, d_bbar + i, d_dots, N);
             device_dot_async(h, rbar, 1.0, vi, 1.0, NVB_DTYPE_F64, d_dots + 1);
@@ -492,9 +499,7 @@ struct Sweep {
                     CK(cudaMemcpyAsync(nat(segv, j - c + 1), cv, per, cudaMemcpyDeviceToDevice, h->stream));
                     segs[j - c + 1] = sc;
                 },
-                [&](int64_t j, const void *w) {
-                    CK(cudaMemcpyAsync(nat(segw, j - c), w, per, cudaMemcpyDeviceToDevice, h->stream));
-                });
+                [&](int64_t, const void *) {});
             reverse_steps(c, e);
             return;
         }
@@ -534,7 +539,7 @@ static bool plan_levels(int64_t n, double vectors, int64_t *L, int64_t *B, int64
             else break;
         }
         const int64_t base = l == 0 ? n : b;
-        const double need = 2.0 * (double)l * (double)b + 2.0 * (double)base + 3.0;
+        const double need = 2.0 * (double)l * (double)b + (double)base + 2.0;
         if (need <= vectors) {
             *L = l;
             *B = b;
@@ -604,8 +609,7 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
     h->bw_plan[2] = W.bmax;
     // base storage and work vectors (no base storage when the forward's record is the base range)
     const size_t nbase = from_record ? 0 : 1;
-    DevBuf segv(nbase * (size_t)(W.bmax + 2) * W.per), segw(nbase * (size_t)(W.bmax + 1) * W.per),
-        b0(nbase * W.per), b1(nbase * W.per), b2(nbase * W.per);
+    DevBuf segv(nbase * (size_t)(W.bmax + 2) * W.per), b0(nbase * W.per), b1(nbase * W.per), b2(nbase * W.per);
     DevBuf vbn(W.per64), vbc(W.per64), vbp(W.per64), rb(W.per64), wb(W.per64), wvb(W.per64), c0(W.per64),
         c1(W.per64), c2(W.per64), cw(W.per64);
     const bool h32 = sweep_hv_f32(h);
@@ -613,7 +617,6 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
     W.w32a = (float *)w32a.p;
     W.w32b = (float *)w32b.p;
     W.segv = segv.p;
-    W.segw = segw.p;
     W.segs.assign(W.bmax + 2, 0.0);
     W.b3[0] = b0.p;
     W.b3[1] = b1.p;
@@ -649,9 +652,8 @@ void lanczos_backward(nvb_handle *h, int64_t n, const double *abar_in, const dou
     std::fill(grad, grad + W.nc, 0.0);
     W.gstep.assign(W.nc, 0.0);
     if (from_record) {
-        // the base range 1..n straight from the record: v_j in slot j, w_j in slot j - 1
+        // the base range 1..n straight from the record: v_j in slot j
         W.segv = h->rec_v;
-        W.segw = h->rec_w;
         CK(cudaMemcpyAsync(W.segs.data(), h->rec_vs, (size_t)(n + 2) * sizeof(double), cudaMemcpyDeviceToHost,
                            h->stream));
         CK(cudaStreamSynchronize(h->stream));

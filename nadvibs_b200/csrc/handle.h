@@ -75,9 +75,9 @@ struct nvb_handle {
     void *ck_buf = nullptr;
     double *ck_scale = nullptr;
     // full record of the forward (ck_k = -1), when it fits the backward budget: v_0 = 0,
-    // v_1..v_{n+1} in native precision with their scales, and w_j = H v_j (j = 1..n), so that
-    // the reverse sweep replays nothing
-    void *rec_v = nullptr, *rec_w = nullptr;
+    // v_1..v_{n+1} in native precision with their scales, so that the reverse sweep replays
+    // nothing (it rebuilds w_j = H v_j from the recurrence)
+    void *rec_v = nullptr;
     double *rec_vs = nullptr;
     int64_t rec_cap = 0, rec_n = 0;
     bool rec_ok = false;
@@ -142,7 +142,7 @@ std::vector<double> seed_weights(const nvb_handle *h);
 void ckpt_reserve(nvb_handle *h, int64_t total_iters);
 void ckpt_save(nvb_handle *h, int64_t it);
 void rec_save_v(nvb_handle *h, int64_t it);  // the full record (checkpoint interval -1)
-void rec_save_w(nvb_handle *h, int64_t it);
+void rec_done(nvb_handle *h, int64_t it);
 void ckpt_free(nvb_handle *h);
 void lanczos_backward(nvb_handle *h, int64_t n, const double *abar, const double *bbar, int64_t k, double *grad);
 int64_t ncoef_of(const nvb_handle *h);

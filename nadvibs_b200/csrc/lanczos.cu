@@ -414,7 +414,7 @@ static void lanczos_iter(nvb_handle *h, int64_t it, int slot) {
     archive_push(h, it);
     if (h->timing) CK(cudaEventRecord(h->ev[3 * slot], h->stream));
     hv_any(h, h->buf[h->cur], h->buf[h->work], dt, h->d_scale + h->cur, h->d_part, &nb);
-    rec_save_w(h, it);  // w_it = H v_it, before pass B turns it into the residual
+    rec_done(h, it);  // the record holds v_it; w_it is rebuilt from the v's in the reverse sweep
     if (h->timing) CK(cudaEventRecord(h->ev[3 * slot + 1], h->stream));
     k_finalize<<<1, FIN_THREADS, 0, h->stream>>>(h->d_part, nb, h->d_alpha + it, 0, nullptr, h->d_status, (int)it);
     if (dt == NVB_DTYPE_F32) passB_launch<float>(h, it, &nb);

@@ -165,15 +165,15 @@ def test_recursive_checkpointing_matches_single_level(precision):
         opts["precision"] = precision
     ref = _gradient(p, theta, n, gE, gI, k=n, record=False, **opts)
     scale = np.abs(ref).max()
-    # vectors needed (2 L B + 2 B + 3): L = 0: 83, L = 1 (B = 7): 31, L = 2 (B = 4): 27
-    for vectors, branching, stored in [(None, n, n), (84, n, n), (32, 7, 7), (28, 4, 4)]:
+    # vectors needed (2 L B + B + 2): L = 0: 42, L = 1 (B = 7): 23, L = 2 (B = 4): 22
+    for vectors, branching, stored in [(None, n, n), (42, n, n), (23, 7, 7), (22, 4, 4)]:
         g, plan = _gradient_with_budget(p, theta, n, gE, gI, vectors, precision=precision)
         assert plan["top_interval"] == 0 and plan["stored_range"] == stored, (vectors, plan)
         assert plan["branching"] == branching, (vectors, plan)
         assert np.abs(g - ref).max() <= 1e-12 * scale, (vectors, plan)
     # replays: depth 0 one pass (n - 1 H.v), depth 2 about three passes
-    _, p0 = _gradient_with_budget(p, theta, n, gE, gI, 84, precision=precision)
-    _, p2 = _gradient_with_budget(p, theta, n, gE, gI, 28, precision=precision)
+    _, p0 = _gradient_with_budget(p, theta, n, gE, gI, 42, precision=precision)
+    _, p2 = _gradient_with_budget(p, theta, n, gE, gI, 22, precision=precision)
     assert p0["replayed_hv"] == n and 2 * n < p2["replayed_hv"] <= 3 * n, (p0, p2)
     # the forward's recorded pairs become the top level
     g, plan = _gradient_with_budget(p, theta, n, gE, gI, 32, record_k=10, precision=precision)
