@@ -344,11 +344,12 @@ __global__ void k_gram_reduce(const double *__restrict__ part, int ng, int nout,
 // tables in shared memory), then each warp runs its blocks' MMAs over the tile.  Block partials
 // are summed in a fixed order.
 
-constexpr int G3_THREADS = 512;
+constexpr int G3_THREADS = 640;
 constexpr int G3_NBW = 8;  // most MMA blocks per warp
 constexpr int G3_SMAX = 4; // most electronic states
 
-// Shared-memory column positions of the ordr-3 Gram columns (A as logical; B regrouped).
+// Shared-memory column positions of the ordr-3 Gram columns: A = [X u, x^2 u, u] padded to 8;
+// B regrouped.
 struct G3Pos {
     int nA8, XO, PO, nB8;
     __host__ __device__ G3Pos(int S, int M) {
@@ -475,11 +476,11 @@ __global__ void __launch_bounds__(G3_THREADS, 1)
                     if (m3) x3v += E33[d - 3] * (double)vr[-3 * sh];
                     const int c = k * S + s;
                     if (k == 0) {
-                        sA[s * PT + e] = u0;
+                        sA[(2 * MS + s) * PT + e] = u0;
                         sB[(ps.XO + s) * PT + e] = v0;
                     }
-                    sA[(S + c) * PT + e] = xu;
-                    sA[(S + MS + c) * PT + e] = x2u;
+                    sA[c * PT + e] = xu;
+                    sA[(MS + c) * PT + e] = x2u;
                     sB[c * PT + e] = xv;
                     sB[(ps.XO + S + c) * PT + e] = x2v;
                     sB[(ps.XO + S + MS + c) * PT + e] = ((double)d + 0.5) * v0;
@@ -566,11 +567,11 @@ __global__ void __launch_bounds__(G3_THREADS, 1)
                 const double x3v = e31p * g[hr][3] + e31m * g[hr][5] + e33p * g[hr][10] + e33m * g[hr][11];
                 const int c = k * S + s;
                 if (k == 0) {
-                    sA[s * PT + e] = u0;
+                    sA[(2 * MS + s) * PT + e] = u0;
                     sB[(ps.XO + s) * PT + e] = v0;
                 }
-                sA[(S + c) * PT + e] = xu;
-                sA[(S + MS + c) * PT + e] = x2u;
+                sA[c * PT + e] = xu;
+                sA[(MS + c) * PT + e] = x2u;
                 sB[c * PT + e] = xv;
                 sB[(ps.XO + S + c) * PT + e] = x2v;
                 sB[(ps.XO + S + MS + c) * PT + e] = ((double)d + 0.5) * v0;
@@ -686,7 +687,9 @@ struct G3Cols {
     int x3v(int k, int b) const { return S + 3 * MS + k * S + b; }
     int pair(int l, int m) const { return l * M - l * (l + 1) / 2 + (m - l - 1); }  // l < m
     int XXv(int l, int m, int b) const { return S + 4 * MS + pair(l, m) * S + b; }
-    // shared-memory position (G3Pos) of a B column
+    // shared-memory positions (G3Pos) of an A column (X u, x^2 u, then u: the u columns, which
+    // alone need v, x^2 v, (n+1/2) v and x^3 v, share one 8-column block) and of a B column
+    int posA(int ia) const { return ia < S ? 2 * MS + ia : ia - S; }
     int posB(int jb) const {
         const G3Pos p(S, M);
         if (jb < S) return p.XO + jb;                                  // v
@@ -732,7 +735,7 @@ static void gram3_blocks(int S, int M, std::vector<int> &blocks, std::vector<int
         }
     const int nbA = p.nA8 / 8, nbB = p.nB8 / 8;
     std::vector<int> bno((size_t)nbA * nbB, -1);
-    for (auto &e : need) bno[(size_t)(e.first / 8) * nbB + c.posB(e.second) / 8] = 0;
+    for (auto &e : need) bno[(size_t)(c.posA(e.first) / 8) * nbB + c.posB(e.second) / 8] = 0;
     blocks.clear();
     for (int i = 0; i < nbA; ++i)
         for (int j = 0; j < nbB; ++j)
@@ -742,9 +745,8 @@ static void gram3_blocks(int S, int M, std::vector<int> &blocks, std::vector<int
             }
     index.assign((size_t)c.nA * c.nB, -1);
     for (auto &e : need) {
-        const int pb = c.posB(e.second);
-        index[(size_t)e.first * c.nB + e.second] =
-            64 * bno[(size_t)(e.first / 8) * nbB + pb / 8] + 8 * (e.first % 8) + pb % 8;
+        const int pa = c.posA(e.first), pb = c.posB(e.second);
+        index[(size_t)e.first * c.nB + e.second] = 64 * bno[(size_t)(pa / 8) * nbB + pb / 8] + 8 * (pa % 8) + pb % 8;
     }
 }
 
