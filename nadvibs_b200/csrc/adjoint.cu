@@ -620,12 +620,19 @@ __global__ void __launch_bounds__(G3_THREADS, 1)
         }
     };
     // MMA steps [k0, k1) (four rows each) of a column tile
+    // (a warp's blocks run A-block major: a block with the same A block as the one before it
+    // reuses its A fragment)
     auto mma = [&](const double *cols, int k0, int k1) {
         if (nq == 0) return;
-        for (int kk = k0; kk < k1; ++kk)
+        for (int kk = k0; kk < k1; ++kk) {
+            double a = 0.0;
 #pragma unroll
             for (int q = 0; q < NBW; ++q)
-                if (q < nq) mma_f64_884(acc[q], cols[aoff[q] + 4 * kk], cols[boff[q] + 4 * kk]);
+                if (q < nq) {
+                    if (q == 0 || aoff[q] != aoff[q - 1]) a = cols[aoff[q] + 4 * kk];
+                    mma_f64_884(acc[q], a, cols[boff[q] + 4 * kk]);
+                }
+        }
     };
     __syncthreads();  // tables and strides
     if (ntl > 0) digits(0, sdig0);
