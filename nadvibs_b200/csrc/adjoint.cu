@@ -432,88 +432,8 @@ __global__ void __launch_bounds__(G3_THREADS, 1)
             sdig[i] = r < dimen ? (int)((unsigned)r / (unsigned)ssh[k] % (unsigned)snf[k]) : 0;
         }
     };
-    // columns of tile t: families f < MS the (mode, state) pairs, then the pairs of modes over
-    // all states (each about twelve gathers per row), a lane per row
-    auto expand = [&](int t, const int *sdig, double *sA) {
-        double *sB = sA + ps.nA8 * PT;
-        const long long t0 = first + (long long)t * tstride;
-        for (int f = wid; f < MS + P2; f += nwarp) {
-            if (f < MS) {
-                const int k = f / S, s = f - k * S, nf = snf[k], sh = ssh[k];
-#pragma unroll
-                for (int hr = 0; hr < RPL; ++hr) {
-                    const int e = lane + 32 * hr;
-                    const long long r = t0 + e;
-                    const bool in = r < dimen;
-                    const int d = sdig[k * TR + e];
-                    const bool p1 = in && d + 1 < nf, m1 = in && d >= 1, p2 = in && d + 2 < nf, m2 = in && d >= 2;
-                    const bool p3 = in && d + 3 < nf, m3 = in && d >= 3;
-                    const T *ur = u + (long long)s * dimen + (in ? r : 0), *vr = v + (long long)s * dimen + (in ? r : 0);
-                    const double u0 = in ? (double)ur[0] : 0.0, v0 = in ? (double)vr[0] : 0.0;
-                    const double ed2 = in ? D2[d] : 0.0;
-                    double xu = 0.0, xv = 0.0, x2u = ed2 * u0, x2v = ed2 * v0, x3v = 0.0;
-                    if (p1) {
-                        const double up = (double)ur[sh], vp = (double)vr[sh];
-                        xu += E1[d] * up;
-                        xv += E1[d] * vp;
-                        x3v += E31[d] * vp;
-                    }
-                    if (m1) {
-                        const double um = (double)ur[-sh], vm = (double)vr[-sh];
-                        xu += E1[d - 1] * um;
-                        xv += E1[d - 1] * vm;
-                        x3v += E31[d - 1] * vm;
-                    }
-                    if (p2) {
-                        x2u += E2[d] * (double)ur[2 * sh];
-                        x2v += E2[d] * (double)vr[2 * sh];
-                    }
-                    if (m2) {
-                        x2u += E2[d - 2] * (double)ur[-2 * sh];
-                        x2v += E2[d - 2] * (double)vr[-2 * sh];
-                    }
-                    if (p3) x3v += E33[d] * (double)vr[3 * sh];
-                    if (m3) x3v += E33[d - 3] * (double)vr[-3 * sh];
-                    const int c = k * S + s;
-                    if (k == 0) {
-                        sA[(2 * MS + s) * PT + e] = u0;
-                        sB[(ps.XO + s) * PT + e] = v0;
-                    }
-                    sA[c * PT + e] = xu;
-                    sA[(MS + c) * PT + e] = x2u;
-                    sB[c * PT + e] = xv;
-                    sB[(ps.XO + S + c) * PT + e] = x2v;
-                    sB[(ps.XO + S + MS + c) * PT + e] = ((double)d + 0.5) * v0;
-                    sB[(ps.XO + S + 2 * MS + c) * PT + e] = x3v;
-                }
-            } else {
-                const int pd = f - MS, pw = spair[pd], l = pw & 255, m = pw >> 8;
-                const int nl = snf[l], nm = snf[m], shl = ssh[l], shm = ssh[m];
-#pragma unroll
-                for (int hr = 0; hr < RPL; ++hr) {
-                    const int e = lane + 32 * hr;
-                    const long long r = t0 + e;
-                    const bool in = r < dimen;
-                    const int dl = sdig[l * TR + e], dm = sdig[m * TR + e];
-                    const bool lp = in && dl + 1 < nl, lm = in && dl >= 1, mp = dm + 1 < nm, mm = dm >= 1;
-                    const double elp = lp ? E1[dl] : 0.0, elm = lm ? E1[dl - 1] : 0.0;
-                    const double emp = mp ? E1[dm] : 0.0, emm = mm ? E1[dm - 1] : 0.0;
-                    const bool bpp = lp && mp, bpm = lp && mm, bmp = lm && mp, bmm = lm && mm;
-                    const double cpp = elp * emp, cpm = elp * emm, cmp = elm * emp, cmm = elm * emm;
-                    for (int s = 0; s < S; ++s) {
-                        const T *vr = v + (long long)s * dimen + (in ? r : 0);
-                        double xx = 0.0;
-                        if (bpp) xx += cpp * (double)vr[shl + shm];
-                        if (bpm) xx += cpm * (double)vr[shl - shm];
-                        if (bmp) xx += cmp * (double)vr[shm - shl];
-                        if (bmm) xx += cmm * (double)vr[-shl - shm];
-                        sB[(ps.PO + pd * S + s) * PT + e] = xx;
-                    }
-                }
-            }
-        }
-    };
-    // The same columns one family at a time with a hook between the gathers and their use:
+    // The columns of tile t, one family at a time: families f < MS the (mode, state) pairs, then
+    // the pairs of modes over all states (each about twelve gathers per row), a lane per row.
     // `between()` runs while the family's loads are in flight (the double-buffered schedule puts
     // a slice of the previous tile's MMAs there).  Offsets of neighbours outside the basis are
     // clamped to the row itself and their coefficients are zero, so the loads are unconditional.
@@ -659,7 +579,7 @@ __global__ void __launch_bounds__(G3_THREADS, 1)
         }
     } else {
         for (int i = 0; i < ntl; ++i) {
-            expand(i, sdig0, sm);
+            for (int f = wid; f < MS + P2; f += nwarp) family(f, i, sdig0, sm, [] {});
             __syncthreads();
             mma(sm, 0, TR / 4);
             if (i + 1 < ntl) digits(i + 1, sdig0);
