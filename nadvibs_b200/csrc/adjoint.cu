@@ -336,13 +336,14 @@ __global__ void k_gram_reduce(const double *__restrict__ part, int ng, int nout,
 //   x_k x_l: <X_k u_a, X_l v_b>   x_k^2 x_l: <x_k^2 u_a, X_l v_b>
 //   x_k x_l x_m (k < l < m): <X_k u_a, X_l X_m v_b>,   C = <u_a, v_b>,   K_k = sum_a <u_a, (n_k+1/2) v_a>.
 // The sums over rows run on the FP64 tensor cores (mma m8n8k4): G is cut into 8 x 8 blocks
-// (8 A columns x 8 B columns) and only the blocks holding a needed entry are formed.  The B
-// columns are ordered so that the needed entries cluster: X v first, then v, x^2 v,
-// (n+1/2) v, x^3 v, then X_l X_m v by descending l (an A column X_k u needs exactly the pairs
-// with l > k, a prefix).  Per tile of TR rows the columns are expanded into shared memory
-// (column-major, a warp per mode or pair of modes over all states, a lane per row, element
-// tables in shared memory), then each warp runs its blocks' MMAs over the tile.  Block partials
-// are summed in a fixed order.
+// (8 A columns x 8 B columns) and only the blocks holding a needed entry are formed.  The
+// columns are ordered so that the needed entries cluster: A = [X u, x^2 u, u]; B = X v first,
+// then v, x^2 v, (n+1/2) v, x^3 v, then X_l X_m v by descending l (an A column X_k u needs
+// exactly the pairs with l > k, a prefix).  Per tile of TR rows the columns are expanded into
+// shared memory (column-major, a warp per (mode, state) or per pair of modes over all states, a
+// lane per row, element tables in shared memory), and each warp runs its blocks' MMAs over the
+// tile (over the previous tile, interleaved with its gathers, when two tiles fit).  Block
+// partials are summed in a fixed order.
 
 constexpr int G3_THREADS = 640;
 constexpr int G3_NBW = 8;  // most MMA blocks per warp
